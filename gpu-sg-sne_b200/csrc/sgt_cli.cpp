@@ -1,0 +1,171 @@
+// sgt_cli.cpp -- drop-in for the reference's command line tools
+//   sg_tsne_cuda     (CU/testing_modules/demo_perplexity.cu:32-213)
+//   demo_stochastic_matrix (CU/testing_modules/demo_stochastic_matrix.cu)
+//
+// Usage: sg_tsne_cuda [-d D] [-a alpha] [-m max_iter] [-e early_iter] [-h h]
+//                     [-p np] [-u perplexity] [-f err] [-g ng] [-s sim]
+//                     [-n points] [-t coo|hybrid|csr|2|3|0] [-l lambda]
+//                     [-G fixed|h] [-k kNN-file-is-P: 0|1] FILE
+// FILE holds either a sparse stochastic matrix in Matrix Market coordinate
+// format (1-based "row col value", as buildPFromMTX, CU/utils.cu:335-409) or
+// dense points ("n d" then n*d values, as readXfromMTX, CU/utils.cu:216-256).
+// Dense point input (the kNN stage of the reference) is not part of this
+// build; it reports so and exits.
+// Outputs: sgtsneEmbedding.txt (one point per line) and timeInfo.txt.
+#include "sgtsne_b200.h"
+
+#include <unistd.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+
+static int parse_format(const char *s) {
+  if (!strcmp(s, "coo") || !strcmp(s, "2")) return SGT_FORMAT_COO;
+  if (!strcmp(s, "hybrid") || !strcmp(s, "3")) return SGT_FORMAT_HYBRID;
+  if (!strcmp(s, "csr") || !strcmp(s, "0")) return SGT_FORMAT_CSR;
+  return -1;
+}
+
+static bool read_mtx(const std::string &fn, int &n, std::vector<int> &rp, std::vector<int> &col,
+                     std::vector<float> &val) {
+  std::ifstream fin(fn);
+  if (!fin) return false;
+  std::string line;
+  bool header = false;
+  while (fin.peek() == '%') {
+    std::getline(fin, line);
+    header = true;
+  }
+  (void)header;
+  long m, nn, nnz;
+  if (!(fin >> m >> nn >> nnz)) return false;
+  n = (int)m;
+  std::vector<int> r(nnz), c(nnz);
+  std::vector<float> v(nnz);
+  for (long l = 0; l < nnz; l++)
+    if (!(fin >> r[l] >> c[l] >> v[l])) return false;
+  // column-major input (CSC of the reference) read as rows of P^T: the
+  // reference treats P as column-stochastic; store row = column index.
+  rp.assign(n + 1, 0);
+  for (long l = 0; l < nnz; l++) rp[c[l]]++;
+  for (int i = 0; i < n; i++) rp[i + 1] += rp[i];
+  col.resize(nnz);
+  val.resize(nnz);
+  std::vector<int> fill(rp.begin(), rp.end() - 1);
+  for (long l = 0; l < nnz; l++) {
+    const int cc = c[l] - 1;
+    col[fill[cc]] = r[l] - 1;
+    val[fill[cc]] = v[l];
+    fill[cc]++;
+  }
+  return true;
+}
+
+int main(int argc, char **argv) {
+  if (argc <= 1 || argv[argc - 1][0] == '-') {
+    std::cerr << "No filename provided!" << std::endl;
+    return 1;
+  }
+  std::string filename = argv[argc - 1];
+  sgt_params p;
+  sgt_params_default(&p);
+  float u = 30;
+  int mtx_mode = -1;
+  opterr = 0;
+  int opt;
+  while ((opt = getopt(argc, argv, "d:a:m:e:h:p:u:f:g:s:n:t:l:G:k:")) != -1) {
+    switch (opt) {
+      case 'd': p.d = atoi(optarg); break;
+      case 'm': p.max_iter = atoi(optarg); break;
+      case 'e': p.early_iter = atoi(optarg); break;
+      case 'p': p.np = atoi(optarg); break;
+      case 'u': u = (float)atof(optarg); break;
+      case 'a': p.alpha = (float)atof(optarg); break;
+      case 'h': p.h = (float)atof(optarg); break;
+      case 'f': p.compute_error = atoi(optarg); break;
+      case 'g': p.ng = atoi(optarg); break;
+      case 's': p.sim = atoi(optarg); break;
+      case 'n': p.n = atoi(optarg); break;
+      case 'l': p.lambda = (float)atof(optarg); break;
+      case 't': {
+        const int f = parse_format(optarg);
+        if (f < 0) {
+          std::cerr << "Unknown format: " << optarg << std::endl;
+          return 1;
+        }
+        p.format = f;
+        break;
+      }
+      case 'G': p.grid_mode = !strcmp(optarg, "fixed") ? SGT_GRID_FIXED : SGT_GRID_H; break;
+      case 'k': mtx_mode = atoi(optarg); break;
+      case '?': std::cerr << "Unknown option: '" << char(optopt) << "'!" << std::endl; break;
+    }
+  }
+  sgt_ctx *ctx = nullptr;
+  sgt_status st = sgt_create(0, &ctx);
+  if (st != SGT_OK) {
+    std::cerr << "sgt_create: " << sgt_status_string(st) << std::endl;
+    return 2;
+  }
+  int n = 0;
+  std::vector<int> rp, col;
+  std::vector<float> val;
+  // decide the input kind from the first line: "%" or three numbers = MTX
+  {
+    std::ifstream fin(filename);
+    if (!fin) {
+      std::cerr << "cannot open " << filename << std::endl;
+      return 1;
+    }
+    std::string first;
+    std::getline(fin, first);
+    if (mtx_mode < 0) {
+      std::istringstream is(first);
+      double a, b, c;
+      mtx_mode = (first.size() && first[0] == '%') || (bool)(is >> a >> b >> c);
+    }
+  }
+  if (mtx_mode) {
+    if (!read_mtx(filename, n, rp, col, val)) {
+      std::cerr << "cannot parse matrix " << filename << std::endl;
+      return 1;
+    }
+  } else {
+    std::cerr << "dense point input needs the kNN stage, which this build does not ship;"
+                 " pass a sparse stochastic matrix (Matrix Market)" << std::endl;
+    sgt_destroy(ctx);
+    return 1;
+  }
+  p.n = n;
+  std::vector<float> y((size_t)n * (p.d > 0 ? p.d : 2));
+  std::vector<double> timeinfo(7003, 0.0);
+  st = sgt_embed(ctx, n, rp.data(), col.data(), val.data(), &p, nullptr, y.data(), timeinfo.data());
+  if (st != SGT_OK) {
+    std::cerr << "sgt_embed: " << sgt_status_string(st) << ": " << sgt_last_error(ctx) << std::endl;
+    sgt_destroy(ctx);
+    return 2;
+  }
+  {
+    std::ofstream f("sgtsneEmbedding.txt");
+    for (int i = 0; i < n; i++) {
+      for (int j = 0; j < p.d; j++) f << y[i + (size_t)j * n] << " ";
+      f << "\n";
+    }
+  }
+  {
+    std::ofstream f("timeInfo.txt");
+    f << "total_ms " << timeinfo[7000] << "\nsetup_ms " << timeinfo[7001] << "\nzeta "
+      << timeinfo[7002] << "\n";
+  }
+  printf("time=%lf\n", timeinfo[7000]);
+  sgt_destroy(ctx);
+  return 0;
+}

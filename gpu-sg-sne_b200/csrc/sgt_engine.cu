@@ -1,0 +1,1283 @@
+// sgt_engine.cu -- host side of the engine: the C ABI of include/sgtsne_b200.h.
+//
+// One sgt_job holds an embedding's P, coordinates, momentum, gains, grids and
+// scratch in HBM.  An iteration is captured once as a CUDA graph (fixed
+// launch shapes; every size that changes per iteration is read by the
+// kernels from the device-side SgtState) and replayed max_iter times with no
+// host synchronisation.  Operators (sgt_attractive, sgt_repulsive, ...) run
+// the same kernels on caller buffers for parity tests and for callers that
+// drive the loop themselves.
+#include "../../include/sgtsne_b200.h"
+#include "sgt_common.cuh"
+#include "sgt_fft.cuh"
+#include "sgt_grid.cuh"
+#include "sgt_prep.cuh"
+#include "sgt_rows.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+struct sgt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int nsm = 148;
+  std::string err;
+  sgt_job *scratch = nullptr;  // buffers of the operator entry points
+  int scratch_n = 0, scratch_d = 0;
+  int last_N = 0, last_d = 0;
+};
+
+struct sgt_job {
+  sgt_ctx *ctx = nullptr;
+  sgt_params p{};
+  SgtJobParams jp{};
+  int n = 0, d = 0, S = 1, G = 8, format = SGT_FORMAT_CSR;
+  long nnz = 0;
+  int *rowptr = nullptr;
+  int2 *pairs = nullptr;
+  unsigned *coo_rows = nullptr, *coo_cols = nullptr;
+  float *coo_vals = nullptr;
+  long coo_n = 0;
+  unsigned *ell_cols = nullptr;
+  float *ell_vals = nullptr;
+  int ell_w = 0;
+  float *Y = nullptr, *Ynext = nullptr, *uY = nullptr, *gains = nullptr,
+        *Frep = nullptr, *Fattr = nullptr;
+  float4 *sorted = nullptr;
+  float *V = nullptr, *Phi = nullptr;
+  float2 *W = nullptr;
+  int mmax = 0, nmax = 0;
+  int *tile_count = nullptr, *cursor = nullptr;
+  int4 *chunks = nullptr;
+  float4 *part_min = nullptr, *part_max = nullptr;
+  double *part_sum = nullptr, *part_z = nullptr, *part_kl = nullptr;
+  SgtState *st = nullptr;
+  SgtState *st_host = nullptr;
+  int nb_pts = 0, nb_s2g = 0, nb_g2s = 0, nb_fft = 0, nb_row = 0, nb_part = 0;
+  size_t smem_s2g = 0, smem_fft1 = 0, smem_fft2 = 0;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<void *> allocs;
+  double last_kl = 0.0;
+};
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+static sgt_status fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return s;
+}
+#define CK(call)                                                              \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? SGT_ERR_NO_MEMORY    \
+                                                       : SGT_ERR_CUDA,        \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+#define CKS(expr)                                                             \
+  do {                                                                        \
+    sgt_status s_ = (expr);                                                   \
+    if (s_ != SGT_OK) return s_;                                              \
+  } while (0)
+
+template <typename T>
+static sgt_status jalloc(sgt_job *J, T **ptr, size_t count) {
+  sgt_ctx *ctx = J->ctx;
+  void *p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(&p, count * sizeof(T)));
+  J->allocs.push_back(p);
+  *ptr = (T *)p;
+  return SGT_OK;
+}
+
+static int grid_blocks(int nsm, int per_sm) { return std::max(1, nsm * std::max(1, per_sm)); }
+
+extern "C" {
+
+void sgt_params_default(sgt_params *p) {
+  memset(p, 0, sizeof(*p));
+  p->d = 2;
+  p->lambda = 1.0f;
+  p->alpha = 12.0f;
+  p->max_iter = 1000;
+  p->early_iter = 250;
+  p->n = 0;
+  p->h = -1.0f;
+  p->format = SGT_FORMAT_COO;
+  p->compute_error = -1;
+  p->ng = 50;
+  p->grid_mode = SGT_GRID_H;
+  p->lambda_dist = 1;
+  p->seed = 0;
+}
+
+int sgt_abi_version(void) { return SGT_ABI_VERSION; }
+
+const char *sgt_status_string(sgt_status s) {
+  switch (s) {
+    case SGT_OK: return "ok";
+    case SGT_ERR_INVALID_ARG: return "invalid argument";
+    case SGT_ERR_CUDA: return "CUDA error";
+    case SGT_ERR_NO_MEMORY: return "out of memory";
+    case SGT_ERR_UNSUPPORTED: return "unsupported";
+    case SGT_ERR_NUMERIC: return "non-finite values";
+    case SGT_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown";
+}
+
+int sgt_best_grid_size(int ng) {
+  static const int sizes[137] = {
+      8,   9,   10,  11,  12,  13,  14,  15,  16,  20,  25,  26,  28,  32,  33,
+      35,  36,  39,  40,  42,  44,  45,  48,  49,  50,  52,  54,  55,  56,  60,
+      63,  64,  65,  66,  70,  72,  75,  77,  78,  80,  84,  88,  90,  91,  96,
+      98,  99,  100, 104, 105, 108, 110, 112, 117, 120, 125, 126, 130, 132, 135,
+      140, 144, 147, 150, 154, 156, 160, 165, 168, 175, 176, 180, 182, 189, 192,
+      195, 196, 198, 200, 208, 210, 216, 220, 224, 225, 231, 234, 240, 245, 250,
+      252, 260, 264, 270, 273, 275, 280, 288, 294, 297, 300, 308, 312, 315, 320,
+      325, 330, 336, 343, 350, 351, 352, 360, 364, 375, 378, 385, 390, 392, 396,
+      400, 416, 420, 432, 440, 441, 448, 450, 455, 462, 468, 480, 490, 495, 500,
+      504, 512};
+  for (int i = 0; i < 137; i++)
+    if (ng + 2 <= sizes[i]) return sizes[i] - 2;
+  return sizes[136] - 2;
+}
+
+sgt_status sgt_create(int device, sgt_ctx **out) {
+  if (!out) return SGT_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return SGT_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = new sgt_ctx();
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return SGT_ERR_CUDA;
+  }
+  ctx->own_stream = true;
+  *out = ctx;
+  return SGT_OK;
+}
+
+void sgt_job_destroy(sgt_job *job);
+
+void sgt_destroy(sgt_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->scratch) sgt_job_destroy(ctx->scratch);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+sgt_status sgt_set_stream(sgt_ctx *ctx, void *stream) {
+  if (!ctx) return SGT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (ctx->own_stream && ctx->stream) CK(cudaStreamDestroy(ctx->stream));
+  if (stream) {
+    ctx->stream = (cudaStream_t)stream;
+    ctx->own_stream = false;
+  } else {
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  if (ctx->scratch) {
+    sgt_job_destroy(ctx->scratch);
+    ctx->scratch = nullptr;
+  }
+  return SGT_OK;
+}
+
+const char *sgt_last_error(const sgt_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// validation of a CSR structure (host copy)
+// ---------------------------------------------------------------------------
+static sgt_status check_csr(sgt_ctx *ctx, int n, const int *rowptr, const int *col) {
+  if (rowptr[0] != 0) return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr[0] != 0");
+  for (int i = 0; i < n; i++)
+    if (rowptr[i + 1] < rowptr[i])
+      return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr not monotone at row " + std::to_string(i));
+  const long nnz = rowptr[n];
+  for (long t = 0; t < nnz; t++)
+    if (col[t] < 0 || col[t] >= n)
+      return fail(ctx, SGT_ERR_INVALID_ARG, "column out of range at nonzero " + std::to_string(t));
+  return SGT_OK;
+}
+
+static int choose_group(long nnz, int n) {
+  const double avg = n > 0 ? (double)nnz / n : 0.0;
+  if (avg <= 6) return 4;
+  if (avg <= 20) return 8;
+  if (avg <= 72) return 16;
+  return 32;
+}
+
+// ---------------------------------------------------------------------------
+// job creation
+// ---------------------------------------------------------------------------
+template <int D>
+static sgt_status job_shapes(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
+  const int nsm = ctx->nsm;
+  int occ = 0;
+  J->nb_pts = grid_blocks(nsm, 4);
+  const int T = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  const int R = T + 3;
+  J->smem_s2g = sizeof(float) * (D + 1) * (size_t)(D == 1 ? R : (D == 2 ? R * R : R * R * R));
+  CK(cudaFuncSetAttribute(k_s2g<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_s2g));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g<D>, SGT_THREADS, J->smem_s2g));
+  J->nb_s2g = grid_blocks(nsm, occ);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2s<D>, SGT_THREADS, 0));
+  J->nb_g2s = grid_blocks(nsm, occ);
+  const int M = J->mmax;
+  J->smem_fft1 = sizeof(float2) * (512 + (size_t)SGT_FFT_LINES * (M + 1));
+  J->smem_fft2 = sizeof(float2) * (512 + 2 * (size_t)SGT_FFT_LINES * (M + 1));
+  if constexpr (D == 1) {
+    J->smem_fft2 = sizeof(float2) * (512 + 2 * (size_t)(M + 1));
+    CK(cudaFuncSetAttribute(k_conv1d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+    J->nb_fft = 1;
+  } else {
+    CK(cudaFuncSetAttribute(k_fft_build_x<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft1));
+    CK(cudaFuncSetAttribute(k_fft_last<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+    CK(cudaFuncSetAttribute(k_fft_final_x<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+    if constexpr (D == 3)
+      CK(cudaFuncSetAttribute(k_fft_mid_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fft_last<D>, SGT_THREADS, J->smem_fft2));
+    J->nb_fft = grid_blocks(nsm, occ);
+  }
+  occ = 0;
+  switch (J->G) {
+    case 4: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 4, true>, SGT_THREADS, 0)); break;
+    case 8: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 8, true>, SGT_THREADS, 0)); break;
+    case 16: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 16, true>, SGT_THREADS, 0)); break;
+    default: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 32, true>, SGT_THREADS, 0)); break;
+  }
+  J->nb_row = grid_blocks(nsm, occ);
+  J->nb_part = std::max(std::max(J->nb_pts, J->nb_row), std::max(J->nb_g2s, J->nb_s2g));
+  return SGT_OK;
+}
+
+static sgt_status job_alloc(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
+  const int D = J->d;
+  J->S = D == 3 ? 4 : D;
+  const size_t np = (size_t)J->n * J->S;
+  CKS(jalloc(J, &J->Y, np));
+  CKS(jalloc(J, &J->Ynext, np));
+  CKS(jalloc(J, &J->uY, np));
+  CKS(jalloc(J, &J->gains, np));
+  CKS(jalloc(J, &J->Frep, np));
+  CKS(jalloc(J, &J->sorted, (size_t)J->n));
+  int max_grid = J->p.max_grid > 0 ? J->p.max_grid : (D <= 2 ? 512 : 128);
+  // 3-D: at most 256 points per axis (tile histogram of 16^3 entries,
+  // FFT planes of 512^3)
+  max_grid = std::min(D == 3 ? 256 : 512, std::max(16, max_grid));
+  int M = 1;
+  while (M < 2 * max_grid - 1) M <<= 1;
+  if (D == 1) M = std::max(M, 32);
+  J->mmax = M;
+  J->nmax = std::min(512, (M + 1) / 2);
+  size_t nodes = J->nmax;
+  if (D >= 2) nodes *= J->nmax;
+  if (D >= 3) nodes *= J->nmax;
+  const int ncomp = D == 1 ? 2 : 4;
+  CKS(jalloc(J, &J->V, nodes * ncomp));
+  CKS(jalloc(J, &J->Phi, nodes * ncomp));
+  size_t plane = M;
+  if (D >= 2) plane *= M;
+  if (D >= 3) plane *= M;
+  if (D >= 2) CKS(jalloc(J, &J->W, 3 * plane));
+  CKS(jalloc(J, &J->tile_count, SGT_HIST_MAX));
+  CKS(jalloc(J, &J->cursor, SGT_HIST_MAX));
+  J->jp.chunk_cap = J->n / 1024 + SGT_HIST_MAX + 16;
+  CKS(jalloc(J, &J->chunks, (size_t)J->jp.chunk_cap));
+  J->jp.mmax = M;
+  J->jp.tile_cap = SGT_HIST_MAX;
+  CKS(jalloc(J, &J->st, 1));
+  CK(cudaMallocHost((void **)&J->st_host, sizeof(SgtState)));
+  CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, ctx->stream));
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), ctx->stream));
+  return SGT_OK;
+}
+
+static sgt_status job_alloc_parts(sgt_job *J) {
+  CKS(jalloc(J, &J->part_min, (size_t)J->nb_part));
+  CKS(jalloc(J, &J->part_max, (size_t)J->nb_part));
+  CKS(jalloc(J, &J->part_sum, (size_t)J->nb_part * 4));
+  CKS(jalloc(J, &J->part_z, (size_t)J->nb_part));
+  CKS(jalloc(J, &J->part_kl, (size_t)J->nb_part));
+  return SGT_OK;
+}
+
+static void fill_jp(sgt_job *J) {
+  const sgt_params &p = J->p;
+  J->jp.n = J->n;
+  J->jp.d = J->d;
+  J->jp.grid_mode = p.grid_mode;
+  J->jp.n1_fixed = sgt_best_grid_size(p.ng > 0 ? p.ng : 50);
+  float h = p.h;
+  if (h <= 0) h = J->d == 1 ? 0.5f : (J->d == 2 ? 0.7f : 1.2f);
+  J->jp.h = h;
+  J->jp.alpha0 = p.alpha;
+  J->jp.early_iter = p.early_iter;
+  J->jp.mom_switch = 250;
+  J->jp.eta = 200.0f;
+}
+
+// empty scratch job for operator calls (no P)
+static sgt_status job_new(sgt_ctx *ctx, const sgt_params *p, int n, sgt_job **out) {
+  sgt_job *J = new sgt_job();
+  J->ctx = ctx;
+  J->p = *p;
+  J->n = n;
+  J->d = p->d;
+  J->format = p->format;
+  fill_jp(J);
+  sgt_status s = job_alloc(J);
+  if (s == SGT_OK) {
+    switch (J->d) {
+      case 1: s = job_shapes<1>(J); break;
+      case 2: s = job_shapes<2>(J); break;
+      default: s = job_shapes<3>(J); break;
+    }
+  }
+  if (s == SGT_OK) s = job_alloc_parts(J);
+  if (s != SGT_OK) {
+    sgt_job_destroy(J);
+    return s;
+  }
+  *out = J;
+  return SGT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// iteration enqueue
+// ---------------------------------------------------------------------------
+template <int D>
+static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  typedef typename Vec<D>::T VT;
+  typedef typename Node<D>::T NT;
+  const int n = J->n;
+  k_bin_count<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, n,
+                                                   J->st, J->tile_count, (NT *)J->V, 1);
+  k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
+  k_bin_scatter<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, n, J->st, J->cursor,
+                                                     J->sorted);
+  k_s2g<D><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+  if constexpr (D == 1) {
+    k_conv1d<<<1, SGT_THREADS, J->smem_fft2, s>>>(J->st, (const float2 *)J->V, (float2 *)J->Phi);
+  } else {
+    k_fft_build_x<D><<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, (const NT *)J->V, J->W);
+    if constexpr (D == 3) k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 0);
+    k_fft_last<D><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+    if constexpr (D == 3) k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 1);
+    k_fft_final_x<D><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W, (NT *)J->Phi);
+  }
+  k_g2s<D><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi,
+                                             (VT *)J->Frep, J->part_z, n);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+template <int D, int G>
+static sgt_status enqueue_update(sgt_job *J, cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  typedef typename Vec<D>::T VT;
+  const int n = J->n;
+  if (J->format == SGT_FORMAT_CSR) {
+    k_row_update<D, G, true><<<J->nb_row, SGT_THREADS, 0, s>>>(
+        J->rowptr, J->pairs, nullptr, (const VT *)J->Y, (const VT *)J->Frep, (VT *)J->uY,
+        (VT *)J->gains, (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max, J->part_sum);
+  } else {
+    if (J->format == SGT_FORMAT_HYBRID) {
+      k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals,
+                                                      (const VT *)J->Y, (VT *)J->Fattr);
+    } else {
+      CK(cudaMemsetAsync(J->Fattr, 0, sizeof(float) * (size_t)n * J->S, s));
+    }
+    if (J->coo_n > 0)
+      k_attr_coo<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(J->coo_n, J->coo_rows, J->coo_cols,
+                                                      J->coo_vals, (const VT *)J->Y, J->Fattr);
+    k_row_update<D, G, false><<<J->nb_row, SGT_THREADS, 0, s>>>(
+        nullptr, nullptr, (const VT *)J->Fattr, (const VT *)J->Y, (const VT *)J->Frep,
+        (VT *)J->uY, (VT *)J->gains, (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max,
+        J->part_sum);
+  }
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+template <int D>
+static sgt_status enqueue_iteration(sgt_job *J, cudaStream_t s) {
+  CKS(enqueue_repulsion<D>(J, s));
+  switch (J->G) {
+    case 4: return enqueue_update<D, 4>(J, s);
+    case 8: return enqueue_update<D, 8>(J, s);
+    case 16: return enqueue_update<D, 16>(J, s);
+    default: return enqueue_update<D, 32>(J, s);
+  }
+}
+
+static sgt_status dispatch_iteration(sgt_job *J, cudaStream_t s) {
+  switch (J->d) {
+    case 1: return enqueue_iteration<1>(J, s);
+    case 2: return enqueue_iteration<2>(J, s);
+    default: return enqueue_iteration<3>(J, s);
+  }
+}
+
+template <int D>
+static sgt_status enqueue_init_stats(sgt_job *J, cudaStream_t s, int centre) {
+  sgt_ctx *ctx = J->ctx;
+  k_init_stats<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const typename Vec<D>::T *)J->Ynext, J->n,
+                                                    J->st, J->jp, J->part_min, J->part_max,
+                                                    J->part_sum, centre);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+static sgt_status init_stats(sgt_job *J, cudaStream_t s, int centre) {
+  switch (J->d) {
+    case 1: return enqueue_init_stats<1>(J, s, centre);
+    case 2: return enqueue_init_stats<2>(J, s, centre);
+    default: return enqueue_init_stats<3>(J, s, centre);
+  }
+}
+
+static sgt_status pack_y(sgt_job *J, const float *src, int layout, float *dst, cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  const int nb = grid_blocks(ctx->nsm, 4);
+  const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+  switch (J->d) {
+    case 1: k_pack<1><<<nb, SGT_THREADS, 0, s>>>(src, J->n, dm, (float *)dst); break;
+    case 2: k_pack<2><<<nb, SGT_THREADS, 0, s>>>(src, J->n, dm, (float2 *)dst); break;
+    default: k_pack<3><<<nb, SGT_THREADS, 0, s>>>(src, J->n, dm, (float4 *)dst); break;
+  }
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+template <int D>
+__global__ void k_unpack_divz(const typename Vec<D>::T *__restrict__ src, int n, int dim_major,
+                              const SgtState *st, float *__restrict__ dst) {
+  const float z = (float)st->Z;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const typename Vec<D>::T v = src[i];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      const float x = comp<D>(v, k) / z;
+      if (dim_major) dst[i + (long)k * n] = x; else dst[(long)i * D + k] = x;
+    }
+  }
+}
+
+template <int D>
+__global__ void k_write_bins(const typename Vec<D>::T *__restrict__ Y, int n,
+                             const SgtState *st, uint32_t *__restrict__ bins) {
+  const float maxy = st->maxy, scale = st->scale;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const typename Vec<D>::T y = Y[i];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      float sh;
+      bins[(long)i * D + k] = (uint32_t)floorf(sgt_scale(comp<D>(y, k), st->miny[k], maxy, scale, sh));
+    }
+  }
+}
+
+// mean of the current coordinates subtracted on the way out
+template <int D>
+__global__ void k_unpack_centred(const typename Vec<D>::T *__restrict__ src, int n, int dim_major,
+                                 const SgtState *st, int use_next_mean, float *__restrict__ dst) {
+  float mean[3];
+  for (int k = 0; k < D; k++) mean[k] = use_next_mean ? (float)(st->sum[k] / (double)n) : 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const typename Vec<D>::T v = src[i];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      const float x = comp<D>(v, k) - mean[k];
+      if (dim_major) dst[i + (long)k * n] = x; else dst[(long)i * D + k] = x;
+    }
+  }
+}
+
+static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int ng, float h) {
+  if (!ctx->scratch || ctx->scratch_n < n || ctx->scratch_d != d) {
+    if (ctx->scratch) sgt_job_destroy(ctx->scratch);
+    ctx->scratch = nullptr;
+    sgt_params p;
+    sgt_params_default(&p);
+    p.d = d;
+    p.format = SGT_FORMAT_CSR;
+    CKS(job_new(ctx, &p, n, &ctx->scratch));
+    ctx->scratch_n = n;
+    ctx->scratch_d = d;
+  }
+  sgt_job *J = ctx->scratch;
+  J->n = n;
+  J->jp.n = n;
+  J->p.grid_mode = grid_mode;
+  J->jp.grid_mode = grid_mode;
+  J->jp.n1_fixed = sgt_best_grid_size(ng > 0 ? ng : 50);
+  J->jp.h = h > 0 ? h : (d == 1 ? 0.5f : (d == 2 ? 0.7f : 1.2f));
+  return SGT_OK;
+}
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// jobs
+// ---------------------------------------------------------------------------
+sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const int *rowptr,
+                          const int *col, const float *val, int mem_is_device, sgt_job **out) {
+  if (!ctx || !params || !rowptr || !col || !val || !out) return SGT_ERR_INVALID_ARG;
+  if (n < 2) return fail(ctx, SGT_ERR_INVALID_ARG, "need at least 2 points");
+  if (params->d < 1 || params->d > 3) return fail(ctx, SGT_ERR_UNSUPPORTED, "d must be 1, 2 or 3");
+  if (params->format != SGT_FORMAT_CSR && params->format != SGT_FORMAT_COO &&
+      params->format != SGT_FORMAT_HYBRID)
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "format must be 0 (csr), 2 (coo) or 3 (hybrid)");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  // host copy of the structure (validation, formats)
+  std::vector<int> hrp(n + 1);
+  if (mem_is_device) {
+    CK(cudaMemcpyAsync(hrp.data(), rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  } else {
+    memcpy(hrp.data(), rowptr, sizeof(int) * (n + 1));
+  }
+  const long nnz = hrp[n];
+  if (nnz <= 0) return fail(ctx, SGT_ERR_INVALID_ARG, "P has no nonzeros");
+  std::vector<int> hcol;
+  std::vector<float> hval;
+  const bool need_host = !mem_is_device || params->format == SGT_FORMAT_HYBRID;
+  if (mem_is_device) {
+    if (params->format == SGT_FORMAT_HYBRID) {
+      hcol.resize(nnz);
+      hval.resize(nnz);
+      CK(cudaMemcpyAsync(hcol.data(), col, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(hval.data(), val, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      CKS(check_csr(ctx, n, hrp.data(), hcol.data()));
+    }
+  } else {
+    CKS(check_csr(ctx, n, hrp.data(), col));
+  }
+  (void)need_host;
+  if (mem_is_device && params->format != SGT_FORMAT_HYBRID) {
+    int *bad = nullptr;
+    CK(cudaMalloc(&bad, sizeof(int)));
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    k_validate_csr<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(n, rowptr, col, bad);
+    int hb = 0;
+    CK(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    cudaFree(bad);
+    if (hb) return fail(ctx, SGT_ERR_INVALID_ARG, "malformed CSR (rowptr order or column range)");
+  }
+  sgt_job *J = new sgt_job();
+  J->ctx = ctx;
+  J->p = *params;
+  J->p.n = n;
+  J->n = n;
+  J->d = params->d;
+  J->nnz = nnz;
+  J->format = params->format;
+  J->G = choose_group(nnz, n);
+  fill_jp(J);
+  sgt_status st = job_alloc(J);
+  if (st == SGT_OK) {
+    switch (J->d) {
+      case 1: st = job_shapes<1>(J); break;
+      case 2: st = job_shapes<2>(J); break;
+      default: st = job_shapes<3>(J); break;
+    }
+  }
+  if (st == SGT_OK) st = job_alloc_parts(J);
+  if (st != SGT_OK) {
+    sgt_job_destroy(J);
+    return st;
+  }
+  auto bail = [&](sgt_status e) {
+    sgt_job_destroy(J);
+    return e;
+  };
+  // P on the device in the chosen format
+  int *dcol = nullptr;
+  float *dval = nullptr;
+  st = jalloc(J, &J->rowptr, (size_t)n + 1);
+  if (st != SGT_OK) return bail(st);
+  if (J->format == SGT_FORMAT_CSR) {
+    st = jalloc(J, &J->pairs, (size_t)nnz);
+    if (st != SGT_OK) return bail(st);
+  }
+  const cudaMemcpyKind kind = mem_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (cudaMemcpyAsync(J->rowptr, rowptr, sizeof(int) * (n + 1), kind, s) != cudaSuccess)
+    return bail(fail(ctx, SGT_ERR_CUDA, "copy rowptr"));
+  if (J->format == SGT_FORMAT_CSR || J->format == SGT_FORMAT_COO) {
+    if (mem_is_device) {
+      dcol = (int *)col;
+      dval = (float *)val;
+    } else {
+      if (cudaMalloc(&dcol, sizeof(int) * nnz) != cudaSuccess ||
+          cudaMalloc(&dval, sizeof(float) * nnz) != cudaSuccess)
+        return bail(fail(ctx, SGT_ERR_NO_MEMORY, "staging P"));
+      cudaMemcpyAsync(dcol, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(dval, val, sizeof(float) * nnz, cudaMemcpyHostToDevice, s);
+    }
+    if (J->format == SGT_FORMAT_CSR) {
+      k_pack_pairs<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, s>>>(nnz, dcol, dval, J->pairs);
+    } else {
+      J->coo_n = nnz;
+      if ((st = jalloc(J, &J->coo_rows, (size_t)nnz)) != SGT_OK ||
+          (st = jalloc(J, &J->coo_cols, (size_t)nnz)) != SGT_OK ||
+          (st = jalloc(J, &J->coo_vals, (size_t)nnz)) != SGT_OK)
+        return bail(st);
+      k_csr_to_coo<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, s>>>(n, nnz, J->rowptr, J->coo_rows);
+      cudaMemcpyAsync(J->coo_cols, dcol, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(J->coo_vals, dval, sizeof(float) * nnz, cudaMemcpyDeviceToDevice, s);
+    }
+    if (cudaGetLastError() != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "packing P"));
+    if (!mem_is_device) {
+      cudaStreamSynchronize(s);
+      cudaFree(dcol);
+      cudaFree(dval);
+    }
+  } else {  // hybrid: host split like CU/prepareMatrix.cu:55-97
+    const int *hc = mem_is_device ? hcol.data() : col;
+    const float *hv = mem_is_device ? hval.data() : val;
+    const int w = sgt_ell_width(n, hrp.data());
+    std::vector<unsigned> ec((size_t)n * std::max(w, 1)), cr(nnz), cc(nnz);
+    std::vector<float> ev((size_t)n * std::max(w, 1)), cv(nnz);
+    long csz = 0;
+    sgt_csr_to_hybrid(n, hrp.data(), hc, hv, w, ec.data(), ev.data(), cr.data(), cc.data(),
+                      cv.data(), &csz);
+    J->ell_w = w;
+    J->coo_n = csz;
+    if ((st = jalloc(J, &J->ell_cols, (size_t)n * std::max(w, 1))) != SGT_OK ||
+        (st = jalloc(J, &J->ell_vals, (size_t)n * std::max(w, 1))) != SGT_OK ||
+        (st = jalloc(J, &J->coo_rows, (size_t)std::max(csz, 1L))) != SGT_OK ||
+        (st = jalloc(J, &J->coo_cols, (size_t)std::max(csz, 1L))) != SGT_OK ||
+        (st = jalloc(J, &J->coo_vals, (size_t)std::max(csz, 1L))) != SGT_OK)
+      return bail(st);
+    cudaMemcpyAsync(J->ell_cols, ec.data(), sizeof(unsigned) * (size_t)n * w, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(J->ell_vals, ev.data(), sizeof(float) * (size_t)n * w, cudaMemcpyHostToDevice, s);
+    if (csz > 0) {
+      cudaMemcpyAsync(J->coo_rows, cr.data(), sizeof(unsigned) * csz, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(J->coo_cols, cc.data(), sizeof(unsigned) * csz, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(J->coo_vals, cv.data(), sizeof(float) * csz, cudaMemcpyHostToDevice, s);
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "hybrid upload"));
+  }
+  if (J->format != SGT_FORMAT_CSR) {
+    if ((st = jalloc(J, &J->Fattr, (size_t)n * J->S)) != SGT_OK) return bail(st);
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "job setup"));
+  *out = J;
+  return SGT_OK;
+}
+
+void sgt_job_destroy(sgt_job *J) {
+  if (!J) return;
+  if (J->ctx) cudaSetDevice(J->ctx->device);
+  if (J->gexec) cudaGraphExecDestroy(J->gexec);
+  for (void *p : J->allocs) cudaFree(p);
+  if (J->st_host) cudaFreeHost(J->st_host);
+  delete J;
+}
+
+sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_device) {
+  if (!J || !y) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t bytes = sizeof(float) * (size_t)J->n * J->d;
+  const float *src = y;
+  float *staging = nullptr;
+  if (!mem_is_device) {
+    CK(cudaMalloc(&staging, bytes));
+    CK(cudaMemcpyAsync(staging, y, bytes, cudaMemcpyHostToDevice, s));
+    src = staging;
+  }
+  CKS(pack_y(J, src, layout, J->Ynext, s));
+  CK(cudaMemsetAsync(J->uY, 0, sizeof(float) * (size_t)J->n * J->S, s));
+  {
+    std::vector<float> ones((size_t)J->n * J->S, 1.0f);
+    CK(cudaMemcpyAsync(J->gains, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
+  CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, s));
+  CKS(init_stats(J, s, J->p.grid_mode == SGT_GRID_H ? 1 : 1));
+  if (staging) {
+    CK(cudaStreamSynchronize(s));
+    CK(cudaFree(staging));
+  }
+  return SGT_OK;
+}
+
+sgt_status sgt_job_run(sgt_job *J, int iters) {
+  if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  if (!J->gexec) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    sgt_status es = dispatch_iteration(J, s);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (es != SGT_OK) {
+      if (g) cudaGraphDestroy(g);
+      return es;
+    }
+    CK(ce);
+    cudaError_t ie = cudaGraphInstantiate(&J->gexec, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+  }
+  const int kl_every = J->p.kl_every;
+  for (int it = 0; it < iters; it++) {
+    CK(cudaGraphLaunch(J->gexec, s));
+    if (kl_every > 0 && ((it + 1) % kl_every) == 0) {
+      double kl = 0;
+      // KL of the coordinates the step just used (Y) with that step's Z
+      sgt_status ks = sgt_job_kl(J, -1.0, &kl);
+      if (ks != SGT_OK) return ks;
+    }
+  }
+  return SGT_OK;
+}
+
+sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, int centre) {
+  if (!J || !y) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t bytes = sizeof(float) * (size_t)J->n * J->d;
+  float *dst = y, *staging = nullptr;
+  if (!mem_is_device) {
+    CK(cudaMalloc(&staging, bytes));
+    dst = staging;
+  }
+  const int nb = grid_blocks(ctx->nsm, 4);
+  const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+  switch (J->d) {
+    case 1: k_unpack_centred<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J->Ynext, J->n, dm, J->st, centre, dst); break;
+    case 2: k_unpack_centred<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J->Ynext, J->n, dm, J->st, centre, dst); break;
+    default: k_unpack_centred<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)J->Ynext, J->n, dm, J->st, centre, dst); break;
+  }
+  CK(cudaGetLastError());
+  if (staging) {
+    CK(cudaMemcpyAsync(y, staging, bytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaFree(staging));
+  } else {
+    CK(cudaStreamSynchronize(s));
+  }
+  return SGT_OK;
+}
+
+sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
+  if (!J || !info) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  info->iter = J->st_host->iter;
+  info->grid_points = J->st_host->N;
+  info->h_eff = J->st_host->h_eff;
+  info->zeta = J->st_host->Z;
+  info->kl = J->last_kl;
+  info->error_flags = J->st_host->error;
+  info->nnz = J->nnz;
+  return SGT_OK;
+}
+
+}  // extern "C"
+
+template <int D, int G>
+static void launch_kl(sgt_job *J, double alpha, cudaStream_t s) {
+  k_kl<D, G><<<J->nb_row, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const typename Vec<D>::T *)J->Y,
+                                               J->st, alpha, J->part_kl, J->n);
+}
+
+extern "C" {
+
+// alpha < 0: the alpha of the last completed iteration
+sgt_status sgt_job_kl(sgt_job *J, double alpha, double *kl) {
+  if (!J || !kl) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  if (J->format != SGT_FORMAT_CSR)
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "KL on a job needs the CSR format");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  if (alpha < 0) {
+    CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    alpha = J->st_host->alpha > 0 ? J->st_host->alpha : J->p.alpha;
+  }
+  switch (J->d * 100 + J->G) {
+#define KLC(DD, GG) case DD * 100 + GG: launch_kl<DD, GG>(J, alpha, s); break;
+    KLC(1, 4) KLC(1, 8) KLC(1, 16) KLC(1, 32)
+    KLC(2, 4) KLC(2, 8) KLC(2, 16) KLC(2, 32)
+    KLC(3, 4) KLC(3, 8) KLC(3, 16) KLC(3, 32)
+#undef KLC
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *kl = J->st_host->kl;
+  J->last_kl = *kl;
+  return SGT_OK;
+}
+
+sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
+  if (!J || !stage_ms || iters < 0) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; i++) CK(cudaEventCreate(&ev[i]));
+  typedef void (*fn_t)(sgt_job *, cudaStream_t);
+  for (int it = 0; it < iters; it++) {
+    // same kernels as the graph, bracketed per stage
+    CK(cudaEventRecord(ev[0], s));
+    switch (J->d) {
+      case 1: {
+        typedef Vec<1>::T VT; typedef Node<1>::T NT;
+        k_bin_count<1><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n, J->st, J->tile_count, (NT *)J->V, 1);
+        k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
+        k_bin_scatter<1><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, J->n, J->st, J->cursor, J->sorted);
+        CK(cudaEventRecord(ev[1], s));
+        k_s2g<1><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+        CK(cudaEventRecord(ev[2], s));
+        k_conv1d<<<1, SGT_THREADS, J->smem_fft2, s>>>(J->st, (const float2 *)J->V, (float2 *)J->Phi);
+        CK(cudaEventRecord(ev[3], s));
+        k_g2s<1><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
+        break;
+      }
+      case 2: {
+        typedef Vec<2>::T VT; typedef Node<2>::T NT;
+        k_bin_count<2><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n, J->st, J->tile_count, (NT *)J->V, 1);
+        k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
+        k_bin_scatter<2><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, J->n, J->st, J->cursor, J->sorted);
+        CK(cudaEventRecord(ev[1], s));
+        k_s2g<2><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+        CK(cudaEventRecord(ev[2], s));
+        k_fft_build_x<2><<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, (const NT *)J->V, J->W);
+        k_fft_last<2><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+        k_fft_final_x<2><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W, (NT *)J->Phi);
+        CK(cudaEventRecord(ev[3], s));
+        k_g2s<2><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
+        break;
+      }
+      default: {
+        typedef Vec<3>::T VT; typedef Node<3>::T NT;
+        k_bin_count<3><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n, J->st, J->tile_count, (NT *)J->V, 1);
+        k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
+        k_bin_scatter<3><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, J->n, J->st, J->cursor, J->sorted);
+        CK(cudaEventRecord(ev[1], s));
+        k_s2g<3><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+        CK(cudaEventRecord(ev[2], s));
+        k_fft_build_x<3><<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, (const NT *)J->V, J->W);
+        k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 0);
+        k_fft_last<3><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+        k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 1);
+        k_fft_final_x<3><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W, (NT *)J->Phi);
+        CK(cudaEventRecord(ev[3], s));
+        k_g2s<3><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
+        break;
+      }
+    }
+    CK(cudaEventRecord(ev[4], s));
+    switch (J->d * 100 + J->G) {
+#define UPC(DD, GG) case DD * 100 + GG: CKS((enqueue_update<DD, GG>(J, s))); break;
+      UPC(1, 4) UPC(1, 8) UPC(1, 16) UPC(1, 32)
+      UPC(2, 4) UPC(2, 8) UPC(2, 16) UPC(2, 32)
+      UPC(3, 4) UPC(3, 8) UPC(3, 16) UPC(3, 32)
+#undef UPC
+    }
+    CK(cudaEventRecord(ev[5], s));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[5]));
+    float ms;
+    for (int k = 0; k < 5; k++) {
+      CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      stage_ms[k] += ms;
+    }
+    CK(cudaEventElapsedTime(&ms, ev[0], ev[5]));
+    stage_ms[5] += ms;
+  }
+  for (int i = 0; i < 6; i++) cudaEventDestroy(ev[i]);
+  return SGT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed, const float *y,
+                         int layout, float *f, double *zeta, int *grid_points, float *h_eff) {
+  if (!ctx || !y || !f) return SGT_ERR_INVALID_ARG;
+  if (n < 2 || d < 1 || d > 3) return fail(ctx, SGT_ERR_INVALID_ARG, "need n >= 2 and 1 <= d <= 3");
+  CK(cudaSetDevice(ctx->device));
+  CKS(ensure_scratch(ctx, n, d, ng_fixed > 0 ? SGT_GRID_FIXED : SGT_GRID_H, ng_fixed, h));
+  sgt_job *J = ctx->scratch;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
+  CKS(pack_y(J, y, layout, J->Ynext, s));
+  CKS(init_stats(J, s, 0));
+  switch (d) {
+    case 1: CKS(enqueue_repulsion<1>(J, s)); break;
+    case 2: CKS(enqueue_repulsion<2>(J, s)); break;
+    default: CKS(enqueue_repulsion<3>(J, s)); break;
+  }
+  const int nb = grid_blocks(ctx->nsm, 4);
+  const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+  switch (d) {
+    case 1: k_unpack_divz<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J->Frep, n, dm, J->st, f); break;
+    case 2: k_unpack_divz<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J->Frep, n, dm, J->st, f); break;
+    default: k_unpack_divz<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)J->Frep, n, dm, J->st, f); break;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (zeta) *zeta = J->st_host->Z;
+  if (grid_points) *grid_points = J->st_host->N;
+  if (h_eff) *h_eff = J->st_host->h_eff;
+  ctx->last_N = J->st_host->N;
+  ctx->last_d = d;
+  if (J->st_host->error & SGT_EFLAG_NONFINITE)
+    return fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates");
+  return SGT_OK;
+}
+
+sgt_status sgt_bins(sgt_ctx *ctx, int n, int d, float h, int ng_fixed, const float *y, int layout,
+                    uint32_t *bins, int *grid_points) {
+  if (!ctx || !y || !bins) return SGT_ERR_INVALID_ARG;
+  if (n < 2 || d < 1 || d > 3) return fail(ctx, SGT_ERR_INVALID_ARG, "need n >= 2 and 1 <= d <= 3");
+  CK(cudaSetDevice(ctx->device));
+  CKS(ensure_scratch(ctx, n, d, ng_fixed > 0 ? SGT_GRID_FIXED : SGT_GRID_H, ng_fixed, h));
+  sgt_job *J = ctx->scratch;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
+  CKS(pack_y(J, y, layout, J->Ynext, s));
+  CKS(init_stats(J, s, 0));
+  const int nb = grid_blocks(ctx->nsm, 4);
+  switch (d) {
+    case 1: k_write_bins<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J->Ynext, n, J->st, bins); break;
+    case 2: k_write_bins<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J->Ynext, n, J->st, bins); break;
+    default: k_write_bins<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)J->Ynext, n, J->st, bins); break;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (grid_points) *grid_points = J->st_host->N;
+  return SGT_OK;
+}
+
+sgt_status sgt_last_grids(sgt_ctx *ctx, float *v_grid, float *phi_grid) {
+  if (!ctx || !ctx->scratch || ctx->last_N <= 0) return fail(ctx, SGT_ERR_INVALID_ARG, "no grids yet");
+  CK(cudaSetDevice(ctx->device));
+  sgt_job *J = ctx->scratch;
+  const int d = ctx->last_d, N = ctx->last_N, m = d + 1, nc = d == 1 ? 2 : 4;
+  size_t nodes = N;
+  if (d >= 2) nodes *= N;
+  if (d >= 3) nodes *= N;
+  std::vector<float> tmp(nodes * nc);
+  float *outs[2] = {v_grid, phi_grid};
+  const float *srcs[2] = {J->V, J->Phi};
+  for (int q = 0; q < 2; q++) {
+    if (!outs[q]) continue;
+    CK(cudaMemcpyAsync(tmp.data(), srcs[q], sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t g = 0; g < nodes; g++)
+      for (int c = 0; c < m; c++) outs[q][c * nodes + g] = tmp[g * nc + c];
+  }
+  return SGT_OK;
+}
+
+sgt_status sgt_attractive(sgt_ctx *ctx, int format, int n, int d, long nnz, const int *rowptr,
+                          const unsigned *coo_rows, const int *col, const float *val,
+                          const float *y, int layout, float *f) {
+  if (!ctx || !col || !val || !y || !f || n < 1 || nnz < 0 || d < 1 || d > 3)
+    return SGT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  sgt_params p;
+  sgt_params_default(&p);
+  p.d = d;
+  p.format = format;
+  sgt_job tmp;  // holds temporary device buffers only
+  tmp.ctx = ctx;
+  tmp.d = d;
+  tmp.n = n;
+  tmp.S = d == 3 ? 4 : d;
+  const int S = tmp.S;
+  sgt_status st = SGT_OK;
+  auto cleanup = [&]() { for (void *q : tmp.allocs) cudaFree(q); tmp.allocs.clear(); };
+  float *Yp = nullptr, *Fp = nullptr;
+  if ((st = jalloc(&tmp, &Yp, (size_t)n * S)) != SGT_OK || (st = jalloc(&tmp, &Fp, (size_t)n * S)) != SGT_OK) {
+    cleanup();
+    return st;
+  }
+  tmp.Y = Yp;
+  st = pack_y(&tmp, y, layout, Yp, s);
+  const int nb = grid_blocks(ctx->nsm, 8);
+  const int G = choose_group(nnz, n);
+  if (st == SGT_OK && format == SGT_FORMAT_CSR) {
+    if (!rowptr) { cleanup(); return SGT_ERR_INVALID_ARG; }
+    int2 *pairs = nullptr;
+    if ((st = jalloc(&tmp, &pairs, (size_t)nnz)) == SGT_OK) {
+      k_pack_pairs<<<nb, SGT_THREADS, 0, s>>>(nnz, col, val, pairs);
+      switch (d * 100 + G) {
+#define ATC(DD, GG) case DD * 100 + GG: k_attr_csr<DD, GG><<<nb, SGT_THREADS, 0, s>>>(rowptr, pairs, (const typename Vec<DD>::T *)Yp, (typename Vec<DD>::T *)Fp, n); break;
+        ATC(1, 4) ATC(1, 8) ATC(1, 16) ATC(1, 32)
+        ATC(2, 4) ATC(2, 8) ATC(2, 16) ATC(2, 32)
+        ATC(3, 4) ATC(3, 8) ATC(3, 16) ATC(3, 32)
+#undef ATC
+      }
+    }
+  } else if (st == SGT_OK && format == SGT_FORMAT_COO) {
+    if (!coo_rows) { cleanup(); return SGT_ERR_INVALID_ARG; }
+    cudaMemsetAsync(Fp, 0, sizeof(float) * (size_t)n * S, s);
+    switch (d) {
+      case 1: k_attr_coo<1><<<nb, SGT_THREADS, 0, s>>>(nnz, coo_rows, (const unsigned *)col, val, (const float *)Yp, Fp); break;
+      case 2: k_attr_coo<2><<<nb, SGT_THREADS, 0, s>>>(nnz, coo_rows, (const unsigned *)col, val, (const float2 *)Yp, Fp); break;
+      default: k_attr_coo<3><<<nb, SGT_THREADS, 0, s>>>(nnz, coo_rows, (const unsigned *)col, val, (const float4 *)Yp, Fp); break;
+    }
+  } else if (st == SGT_OK && format == SGT_FORMAT_HYBRID) {
+    if (!rowptr) { cleanup(); return SGT_ERR_INVALID_ARG; }
+    std::vector<int> hrp(n + 1), hc(nnz);
+    std::vector<float> hv(nnz);
+    cudaMemcpyAsync(hrp.data(), rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hc.data(), col, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hv.data(), val, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s);
+    CK(cudaStreamSynchronize(s));
+    const int w = sgt_ell_width(n, hrp.data());
+    std::vector<unsigned> ec((size_t)n * std::max(w, 1)), cr(std::max(nnz, 1L)), cc(std::max(nnz, 1L));
+    std::vector<float> ev((size_t)n * std::max(w, 1)), cv(std::max(nnz, 1L));
+    long csz = 0;
+    sgt_csr_to_hybrid(n, hrp.data(), hc.data(), hv.data(), w, ec.data(), ev.data(), cr.data(), cc.data(), cv.data(), &csz);
+    unsigned *dec, *dcr, *dcc;
+    float *dev_, *dcv;
+    if ((st = jalloc(&tmp, &dec, ec.size())) == SGT_OK && (st = jalloc(&tmp, &dev_, ev.size())) == SGT_OK &&
+        (st = jalloc(&tmp, &dcr, cr.size())) == SGT_OK && (st = jalloc(&tmp, &dcc, cc.size())) == SGT_OK &&
+        (st = jalloc(&tmp, &dcv, cv.size())) == SGT_OK) {
+      cudaMemcpyAsync(dec, ec.data(), sizeof(unsigned) * ec.size(), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(dev_, ev.data(), sizeof(float) * ev.size(), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(dcr, cr.data(), sizeof(unsigned) * cr.size(), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(dcc, cc.data(), sizeof(unsigned) * cc.size(), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(dcv, cv.data(), sizeof(float) * cv.size(), cudaMemcpyHostToDevice, s);
+      switch (d) {
+        case 1: k_attr_ell<1><<<nb, SGT_THREADS, 0, s>>>(n, w, dec, dev_, (const float *)Yp, (float *)Fp);
+                if (csz) k_attr_coo<1><<<nb, SGT_THREADS, 0, s>>>(csz, dcr, dcc, dcv, (const float *)Yp, Fp); break;
+        case 2: k_attr_ell<2><<<nb, SGT_THREADS, 0, s>>>(n, w, dec, dev_, (const float2 *)Yp, (float2 *)Fp);
+                if (csz) k_attr_coo<2><<<nb, SGT_THREADS, 0, s>>>(csz, dcr, dcc, dcv, (const float2 *)Yp, Fp); break;
+        default: k_attr_ell<3><<<nb, SGT_THREADS, 0, s>>>(n, w, dec, dev_, (const float4 *)Yp, (float4 *)Fp);
+                 if (csz) k_attr_coo<3><<<nb, SGT_THREADS, 0, s>>>(csz, dcr, dcc, dcv, (const float4 *)Yp, Fp); break;
+      }
+      CK(cudaStreamSynchronize(s));
+    }
+  } else if (st == SGT_OK) {
+    cleanup();
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "unknown format");
+  }
+  if (st == SGT_OK) {
+    const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+    switch (d) {
+      case 1: k_unpack<1><<<nb, SGT_THREADS, 0, s>>>((const float *)Fp, n, dm, 1.0f, nullptr, f); break;
+      case 2: k_unpack<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)Fp, n, dm, 1.0f, nullptr, f); break;
+      default: k_unpack<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)Fp, n, dm, 1.0f, nullptr, f); break;
+    }
+    if (cudaGetLastError() != cudaSuccess) st = fail(ctx, SGT_ERR_CUDA, "attractive kernels");
+    else if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(ctx, SGT_ERR_CUDA, "attractive sync");
+  }
+  cleanup();
+  return st;
+}
+
+sgt_status sgt_kl(sgt_ctx *ctx, int n, int d, long nnz, const int *rowptr, const int *col,
+                  const float *val, const float *y, int layout, double alpha, double zeta,
+                  double *kl) {
+  if (!ctx || !rowptr || !col || !val || !y || !kl || n < 1 || d < 1 || d > 3)
+    return SGT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  sgt_job tmp;
+  tmp.ctx = ctx;
+  tmp.d = d;
+  tmp.n = n;
+  tmp.S = d == 3 ? 4 : d;
+  sgt_status st;
+  auto cleanup = [&]() { for (void *q : tmp.allocs) cudaFree(q); tmp.allocs.clear(); };
+  float *Yp;
+  int2 *pairs;
+  SgtState *sd;
+  double *part;
+  const int nb = grid_blocks(ctx->nsm, 8);
+  if ((st = jalloc(&tmp, &Yp, (size_t)n * tmp.S)) != SGT_OK || (st = jalloc(&tmp, &pairs, (size_t)nnz)) != SGT_OK ||
+      (st = jalloc(&tmp, &sd, 1)) != SGT_OK || (st = jalloc(&tmp, &part, (size_t)nb)) != SGT_OK) {
+    cleanup();
+    return st;
+  }
+  SgtState h;
+  memset(&h, 0, sizeof(h));
+  h.Z = zeta;
+  cudaMemcpyAsync(sd, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+  st = pack_y(&tmp, y, layout, Yp, s);
+  k_pack_pairs<<<nb, SGT_THREADS, 0, s>>>(nnz, col, val, pairs);
+  const int G = choose_group(nnz, n);
+  switch (d * 100 + G) {
+#define KLO(DD, GG) case DD * 100 + GG: k_kl<DD, GG><<<nb, SGT_THREADS, 0, s>>>(rowptr, pairs, (const typename Vec<DD>::T *)Yp, sd, alpha, part, n); break;
+    KLO(1, 4) KLO(1, 8) KLO(1, 16) KLO(1, 32)
+    KLO(2, 4) KLO(2, 8) KLO(2, 16) KLO(2, 32)
+    KLO(3, 4) KLO(3, 8) KLO(3, 16) KLO(3, 32)
+#undef KLO
+  }
+  if (cudaGetLastError() != cudaSuccess) {
+    cleanup();
+    return fail(ctx, SGT_ERR_CUDA, "kl kernel");
+  }
+  cudaMemcpyAsync(&h, sd, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    cleanup();
+    return fail(ctx, SGT_ERR_CUDA, "kl sync");
+  }
+  *kl = h.kl;
+  cleanup();
+  return st;
+}
+
+sgt_status sgt_lambda_bisect(sgt_ctx *ctx, int n, const int *rowptr, float *val, float lambda,
+                             int dist, float *sigma) {
+  if (!ctx || !rowptr || !val || n < 1) return SGT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  k_lambda_bisect<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, ctx->stream>>>(
+      n, rowptr, val, (double)lambda, 1e-5, 100, dist, sigma, nullptr);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SGT_OK;
+}
+
+sgt_status sgt_perplexity(sgt_ctx *ctx, int n, int k, const float *dist, float perplexity,
+                          float *p, float *beta) {
+  if (!ctx || !dist || !p || n < 1 || k < 1) return SGT_ERR_INVALID_ARG;
+  if (k > SGT_PERP_MAXK) return fail(ctx, SGT_ERR_UNSUPPORTED, "k > 256");
+  CK(cudaSetDevice(ctx->device));
+  k_perplexity<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, ctx->stream>>>(
+      n, k, dist, (double)perplexity, 1e-5, 200, p, beta);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SGT_OK;
+}
+
+sgt_status sgt_csr_to_coo(sgt_ctx *ctx, int n, long nnz, const int *rowptr, unsigned *rows) {
+  if (!ctx || !rowptr || !rows || n < 1 || nnz < 0) return SGT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  k_csr_to_coo<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, ctx->stream>>>(n, nnz, rowptr, rows);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SGT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// library entry: the flow of sgtsneCUDA (CU/sgtsne.cu:25-129)
+// ---------------------------------------------------------------------------
+extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const int *col,
+                                const float *val, const sgt_params *params, const float *y_in,
+                                float *y_out, double *time_info) {
+  if (!ctx || !rowptr || !col || !val || !params || !y_out) return SGT_ERR_INVALID_ARG;
+  if (n < 2) return fail(ctx, SGT_ERR_INVALID_ARG, "need at least 2 points");
+  sgt_params p = *params;
+  p.n = n;
+  if (p.d < 1 || p.d > 3) return fail(ctx, SGT_ERR_UNSUPPORTED, "d must be 1, 2 or 3");
+  if (p.compute_error > 0)
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "compute_error is not implemented by this engine");
+  // default h per dimension (CU/sgtsne.cu:29-40)
+  if (p.h <= 0) p.h = p.d == 1 ? 0.5f : (p.d == 2 ? 0.7f : 1.2f);
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const auto t0 = std::chrono::steady_clock::now();
+  CKS(check_csr(ctx, n, rowptr, col));
+  const long nnz = rowptr[n];
+  std::vector<float> v(val, val + nnz);
+  // lambda rescaling unless lambda == 1 (CU/sgtsne.cu:51-54)
+  if (p.lambda != 1.0f) {
+    int *drp = nullptr;
+    float *dv = nullptr;
+    CK(cudaMalloc(&drp, sizeof(int) * (n + 1)));
+    CK(cudaMalloc(&dv, sizeof(float) * nnz));
+    CK(cudaMemcpyAsync(drp, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dv, v.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
+    sgt_status ls = sgt_lambda_bisect(ctx, n, drp, dv, p.lambda, p.lambda_dist, nullptr);
+    if (ls == SGT_OK) {
+      CK(cudaMemcpyAsync(v.data(), dv, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    cudaFree(drp);
+    cudaFree(dv);
+    if (ls != SGT_OK) return ls;
+    if (p.drop_leaf)
+      for (int r = 0; r < n; r++)
+        if (rowptr[r + 1] - rowptr[r] == 1) v[rowptr[r]] = 0.f;
+  }
+  // symmetrise (P + P^T)/(2n) (CU/sgtsne.cu:64-65)
+  long snnz = 0;
+  CKS(sgt_symmetrize(n, rowptr, col, v.data(), 1.0f / (2.0f * n), nullptr, nullptr, nullptr, &snnz));
+  std::vector<int> srp(n + 1), sc(snnz);
+  std::vector<float> sv(snnz);
+  CKS(sgt_symmetrize(n, rowptr, col, v.data(), 1.0f / (2.0f * n), srp.data(), sc.data(), sv.data(), &snnz));
+  sgt_job *J = nullptr;
+  CKS(sgt_job_create(ctx, &p, n, srp.data(), sc.data(), sv.data(), 0, &J));
+  // initial coordinates: given, or 1e-4 N(0,1) as generateRandomGaussianCoord
+  // (CU/utils.cu:185-193), dim-major
+  std::vector<float> y0;
+  const float *ysrc = y_in;
+  if (!ysrc) {
+    y0.resize((size_t)n * p.d);
+    std::default_random_engine gen;
+    if (p.seed) gen.seed((unsigned long)p.seed);
+    std::normal_distribution<float> dist(0.0, 1.0);
+    for (size_t i = 0; i < y0.size(); i++) y0[i] = 0.0001 * dist(gen);
+    ysrc = y0.data();
+  }
+  sgt_status st = sgt_job_set_y(J, ysrc, SGT_LAYOUT_DIM_MAJOR, 0);
+  const auto t1 = std::chrono::steady_clock::now();
+  if (st == SGT_OK) st = sgt_job_run(J, p.max_iter);
+  if (st == SGT_OK) st = sgt_job_get_y(J, y_out, SGT_LAYOUT_DIM_MAJOR, 0, 1);
+  const auto t2 = std::chrono::steady_clock::now();
+  if (st == SGT_OK && time_info) {
+    sgt_job_info info;
+    if (sgt_job_get_info(J, &info) == SGT_OK) time_info[7002] = info.zeta;
+    time_info[7000] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    time_info[7001] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  }
+  if (st == SGT_OK) {
+    sgt_job_info info;
+    st = sgt_job_get_info(J, &info);
+    if (st == SGT_OK && (info.error_flags & SGT_EFLAG_NONFINITE))
+      st = fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates during the iterations");
+  }
+  sgt_job_destroy(J);
+  return st;
+}

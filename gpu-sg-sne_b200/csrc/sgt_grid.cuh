@@ -1,0 +1,522 @@
+// sgt_grid.cuh -- repulsive-term kernels: grid decision, point binning,
+// scatter-to-grid (S2G), gather-from-grid (G2S) with the Z reduction.
+//
+// Reference semantics (CU = code/cuda/SG-tSNE-CUDA/src):
+//   min shift (thrust init 100.0)          CU/Frep.cu:96-102
+//   max, h-driven grid size, table lookup  CU/gradient_descend_varGrid.cu:88-92
+//   scale into [0, N-3), clamp 1-FLT_EPS   CU/nuconv.cu:9-36
+//   cubic Lagrange S2G / G2S               CU/gridding.cu:90-338
+//   Z = sum((1+2|y|^2)Phi0 - 2 y.Phi) - n,
+//   F = (y Phi0 - Phi)/Z                   CU/Frep.cu:42-80, HYB/qq.cpp:75-106
+//
+// B200 structure: points are counting-sorted into T^d-cell tiles every
+// iteration; S2G accumulates one tile per chunk of sorted points in shared
+// memory and flushes with vector atomics, so global atomics scale with the
+// grid, not with n*4^d.  Every kernel reads the grid decision from SgtState,
+// so the chain is graph-capturable with fixed launch shapes.
+#pragma once
+#include "sgt_common.cuh"
+
+// ---------------------------------------------------------------------------
+// Grid decision from the stats of the coordinates that the next kernels bin.
+// minv/maxv are per-dim min/max of Ynext, sums its per-dim sums; the
+// coordinates actually binned are Y = Ynext - mean (mean = 0 if !centre).
+// Rounding is monotone, so min/max of the rounded differences equal the
+// rounded differences of min/max: the decision is the one the reference
+// takes on the centred array.
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ void sgt_finalize_grid(SgtState *st, const SgtJobParams &jp,
+                                  const float *minv, const float *maxv,
+                                  const double *sums, bool centre) {
+  float maxy = 0.0f;
+  for (int k = 0; k < D; k++) {
+    const float mean = centre ? (float)(sums[k] / (double)jp.n) : 0.0f;
+    const float lo = __fsub_rn(minv[k], mean);
+    const float hi = __fsub_rn(maxv[k], mean);
+    const float mn = fminf(100.0f, lo);
+    st->mean[k] = mean;
+    st->miny[k] = mn;
+    maxy = fmaxf(maxy, __fsub_rn(hi, mn));
+  }
+  if (!(maxy > 0.0f) || !isfinite(maxy)) {
+    if (!isfinite(maxy)) st->error |= SGT_EFLAG_NONFINITE;
+    maxy = 1.0f;  // all points coincide: any positive extent gives zero force
+  }
+  int n1;
+  if (jp.grid_mode == 1) {
+    n1 = jp.n1_fixed;
+  } else {
+    int ng = (int)ceilf(__fdiv_rn(maxy, jp.h));
+    ng = ng < 14 ? 14 : ng;
+    n1 = sgt_best_grid_size_dev(ng);
+  }
+  int N = n1 + 2;
+  int M = 1, logM = 0;
+  while (M < 2 * N - 1) { M <<= 1; logM++; }
+  if (M > jp.mmax) {  // keep the grid inside the allocated FFT workspace
+    st->error |= SGT_EFLAG_GRID_CLAMP;
+    st->grid_clamped = 1;
+    int i = 136;
+    while (i > 0 && 2 * c_grid_sizes[i] - 1 > jp.mmax) i--;
+    N = c_grid_sizes[i];
+    n1 = N - 2;
+    M = 1; logM = 0;
+    while (M < 2 * N - 1) { M <<= 1; logM++; }
+  }
+  st->maxy = maxy;
+  st->N = N;
+  st->M = M;
+  st->logM = logM;
+  st->scale = (float)(unsigned)(N - 3);
+  st->h_eff = __fdiv_rn(maxy, (float)(n1 - 1) - 1.1920928955078125e-7f);
+  const int T = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  const int cells = n1 - 1;  // floor bins lie in [0, n1-2]
+  const int td = (cells + T - 1) / T;
+  int nt = td;
+  if (D >= 2) nt *= td;
+  if (D >= 3) nt *= td;
+  st->T = T;
+  st->tiles_dim = td;
+  st->ntiles = nt;
+}
+
+// Scaled coordinate exactly as CU/nuconv.cu:9-36: (y - miny)/maxy, clamp to
+// 1-FLT_EPSILON, times (N-3).  Returns the shifted coordinate too.
+__device__ __forceinline__ float sgt_scale(float y, float miny, float maxy,
+                                           float scale, float &shifted) {
+  shifted = __fsub_rn(y, miny);
+  float v = __fdiv_rn(shifted, maxy);
+  if (v >= 1.0f) v = 1.0f - 1.1920928955078125e-7f;
+  return __fmul_rn(v, scale);
+}
+
+template <int D>
+__device__ __forceinline__ int sgt_tile_of(const int *f, int T, int td) {
+  int t = f[0] / T;
+  if (D >= 2) t += td * (f[1] / T);
+  if (D >= 3) t += td * td * (f[2] / T);
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// init: stats of a given coordinate array (first iteration / operator mode)
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_init_stats(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+             SgtJobParams jp, float4 *part_min, float4 *part_max,
+             double *part_sum, int centre) {
+  __shared__ float smin[SGT_THREADS / 32][4], smax[SGT_THREADS / 32][4];
+  __shared__ double ssum[SGT_THREADS / 32][4];
+  __shared__ bool last;
+  float mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  float mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  double sm[4] = {0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const typename Vec<D>::T y = Y[i];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      const float v = comp<D>(y, k);
+      mn[k] = fminf(mn[k], v);
+      mx[k] = fmaxf(mx[k], v);
+      sm[k] += (double)v;
+    }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    mn[k] = warp_min_f(mn[k]);
+    mx[k] = warp_max_f(mx[k]);
+    sm[k] = warp_sum_d(sm[k]);
+    if (l == 0) { smin[w][k] = mn[k]; smax[w][k] = mx[k]; ssum[w][k] = sm[k]; }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float4 a = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+    float4 b = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
+    double s[4] = {0, 0, 0, 0};
+    for (int j = 0; j < SGT_THREADS / 32; j++) {
+      a.x = fminf(a.x, smin[j][0]); b.x = fmaxf(b.x, smax[j][0]); s[0] += ssum[j][0];
+      if (D > 1) { a.y = fminf(a.y, smin[j][1]); b.y = fmaxf(b.y, smax[j][1]); s[1] += ssum[j][1]; }
+      if (D > 2) { a.z = fminf(a.z, smin[j][2]); b.z = fmaxf(b.z, smax[j][2]); s[2] += ssum[j][2]; }
+    }
+    part_min[blockIdx.x] = a;
+    part_max[blockIdx.x] = b;
+    for (int k = 0; k < 4; k++) part_sum[blockIdx.x * 4 + k] = s[k];
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->done_init, 1u);
+    last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    float lo[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+    float hi[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    double s[4] = {0, 0, 0, 0};
+    for (int b = 0; b < (int)gridDim.x; b++) {
+      lo[0] = fminf(lo[0], __ldcg(&part_min[b].x));
+      hi[0] = fmaxf(hi[0], __ldcg(&part_max[b].x));
+      if (D > 1) { lo[1] = fminf(lo[1], __ldcg(&part_min[b].y)); hi[1] = fmaxf(hi[1], __ldcg(&part_max[b].y)); }
+      if (D > 2) { lo[2] = fminf(lo[2], __ldcg(&part_min[b].z)); hi[2] = fmaxf(hi[2], __ldcg(&part_max[b].z)); }
+      for (int k = 0; k < D; k++) s[k] += __ldcg(&part_sum[b * 4 + k]);
+    }
+    for (int k = 0; k < D; k++) { st->minv[k] = lo[k]; st->maxv[k] = hi[k]; st->sum[k] = s[k]; }
+    sgt_finalize_grid<D>(st, jp, lo, hi, s, centre != 0);
+    st->done_init = 0;
+  }
+}
+
+#define SGT_HIST_MAX 4096  // tiles held in shared memory by the binning kernels
+
+// ---------------------------------------------------------------------------
+// bin_count: centre (Y = Ynext - mean), zero the grid V, count points per tile
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
+            typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+            int *__restrict__ tile_count, typename Node<D>::T *__restrict__ V,
+            int write_centred) {
+  __shared__ int hist[SGT_HIST_MAX];
+  const int ntiles = st->ntiles, T = st->T, td = st->tiles_dim, N = st->N;
+  const float maxy = st->maxy, scale = st->scale;
+  float mean[3], miny[3];
+#pragma unroll
+  for (int k = 0; k < D; k++) { mean[k] = st->mean[k]; miny[k] = st->miny[k]; }
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) hist[t] = 0;
+  // zero the grid for this iteration's S2G
+  long nodes = N;
+  if (D >= 2) nodes *= N;
+  if (D >= 3) nodes *= N;
+  typename Node<D>::T z;
+  if constexpr (D == 1) z = make_float2(0.f, 0.f); else z = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < nodes;
+       g += (long)gridDim.x * blockDim.x)
+    V[g] = z;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    typename Vec<D>::T y = Ynext[i];
+    int f[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      const float yc = __fsub_rn(comp<D>(y, k), mean[k]);
+      setcomp<D>(y, k, yc);
+      float sh;
+      const float s = sgt_scale(yc, miny[k], maxy, scale, sh);
+      f[k] = (int)floorf(s);
+    }
+    if (write_centred) Y[i] = y;
+    atomicAdd(&hist[sgt_tile_of<D>(f, T, td)], 1);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+    if (hist[t]) atomicAdd(&tile_count[t], hist[t]);
+}
+
+// ---------------------------------------------------------------------------
+// bin_scan (one CTA of 1024 threads): tile offsets and the chunk work list
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int block_exclusive_scan_1024(int v, int *total) {
+  __shared__ int wsum[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    wsum[lane] = s;
+  }
+  __syncthreads();
+  const int excl = x - v + (w > 0 ? wsum[w - 1] : 0);
+  *total = wsum[31];
+  __syncthreads();
+  return excl;
+}
+
+__global__ void __launch_bounds__(1024)
+k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
+           int *__restrict__ cursor, int4 *__restrict__ chunks, int nblk) {
+  const int ntiles = st->ntiles;
+  // chunk length: about two chunks per persistent CTA, at least 1024 points
+  int chunk = (jp.n + 2 * nblk - 1) / (2 * nblk);
+  chunk = ((chunk + 255) / 256) * 256;
+  if (chunk < 1024) chunk = 1024;
+  const int per = (ntiles + 1023) / 1024;  // <= 4
+  int cnt[4], cpt[4];
+  int mysum = 0, mych = 0;
+  for (int j = 0; j < per; j++) {
+    const int t = threadIdx.x * per + j;
+    cnt[j] = t < ntiles ? tile_count[t] : 0;
+    cpt[j] = (cnt[j] + chunk - 1) / chunk;
+    mysum += cnt[j];
+    mych += cpt[j];
+  }
+  int tot_pts, tot_ch;
+  int base = block_exclusive_scan_1024(mysum, &tot_pts);
+  int cbase = block_exclusive_scan_1024(mych, &tot_ch);
+  for (int j = 0; j < per; j++) {
+    const int t = threadIdx.x * per + j;
+    if (t >= ntiles) break;
+    cursor[t] = base;
+    for (int c = 0; c < cpt[j]; c++) {
+      const int idx = cbase + c;
+      if (idx < jp.chunk_cap) {
+        const int len = min(chunk, cnt[j] - c * chunk);
+        chunks[idx] = make_int4(t, base + c * chunk, len, 0);
+      }
+    }
+    base += cnt[j];
+    cbase += cpt[j];
+    tile_count[t] = 0;  // ready for the next iteration
+  }
+  if (threadIdx.x == 0) {
+    st->chunk = chunk;
+    if (tot_ch > jp.chunk_cap) {
+      st->error |= SGT_EFLAG_CHUNK_OVERFLOW;
+      tot_ch = jp.chunk_cap;
+    }
+    st->nchunks = tot_ch;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// bin_scatter: counting-sort points into tile order.  Each CTA owns a
+// contiguous range; it counts per tile, reserves its slots with one global
+// atomic per touched tile, then places its points.
+// sorted[p] = (y_0, y_1, y_2 | idx) with idx in the .w bits (.z for d <= 2
+// keeps the same slot: idx is always stored in .w).
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_bin_scatter(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+              int *__restrict__ cursor, float4 *__restrict__ sorted) {
+  __shared__ int lc[SGT_HIST_MAX];
+  const int ntiles = st->ntiles, T = st->T, td = st->tiles_dim;
+  const float maxy = st->maxy, scale = st->scale;
+  float miny[3];
+#pragma unroll
+  for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int lo = blockIdx.x * per, hi = min(n, lo + per);
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) lc[t] = 0;
+  __syncthreads();
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const typename Vec<D>::T y = Y[i];
+    int f[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      float sh;
+      f[k] = (int)floorf(sgt_scale(comp<D>(y, k), miny[k], maxy, scale, sh));
+    }
+    atomicAdd(&lc[sgt_tile_of<D>(f, T, td)], 1);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+    if (lc[t]) lc[t] = atomicAdd(&cursor[t], lc[t]);
+  __syncthreads();
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const typename Vec<D>::T y = Y[i];
+    int f[3] = {0, 0, 0};
+    float4 rec = make_float4(0.f, 0.f, 0.f, __int_as_float(i));
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      float sh;
+      const float v = comp<D>(y, k);
+      f[k] = (int)floorf(sgt_scale(v, miny[k], maxy, scale, sh));
+      if (k == 0) rec.x = v; else if (k == 1) rec.y = v; else rec.z = v;
+    }
+    const int pos = atomicAdd(&lc[sgt_tile_of<D>(f, T, td)], 1);
+    sorted[pos] = rec;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// S2G over chunks of sorted points; one shared-memory tile per chunk.
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ void sgt_point_stencil(const float4 &rec,
+                                                  const float *miny, float maxy,
+                                                  float scale, int *f,
+                                                  float (*w)[4], float *ys) {
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    const float v = k == 0 ? rec.x : (k == 1 ? rec.y : rec.z);
+    const float s = sgt_scale(v, miny[k], maxy, scale, ys[k]);
+    sgt_weights(s, f[k], w[k]);
+  }
+}
+
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_s2g(const float4 *__restrict__ sorted, SgtState *st,
+      const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
+  extern __shared__ float acc[];  // [D+1][R^D]
+  const int T = st->T, td = st->tiles_dim, N = st->N, nch = st->nchunks;
+  const float maxy = st->maxy, scale = st->scale;
+  float miny[3];
+#pragma unroll
+  for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  const int R = T + 3;
+  int RD = R;
+  if (D >= 2) RD *= R;
+  if (D >= 3) RD *= R;
+  constexpr int m = D + 1;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int4 ch = chunks[c];
+    int o[3] = {0, 0, 0};
+    o[0] = (ch.x % td) * T;
+    if (D >= 2) o[1] = ((ch.x / td) % td) * T;
+    if (D >= 3) o[2] = (ch.x / (td * td)) * T;
+    for (int e = threadIdx.x; e < m * RD; e += blockDim.x) acc[e] = 0.f;
+    __syncthreads();
+    for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
+      const float4 rec = sorted[j];
+      int f[3];
+      float w[3][4], ys[3];
+      sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
+      const int l0 = f[0] - o[0];
+      const int l1 = D >= 2 ? f[1] - o[1] : 0;
+      const int l2 = D >= 3 ? f[2] - o[2] : 0;
+      // a point outside its tile would mean the sort and the binning
+      // disagree; skip it rather than touch memory outside the tile
+      if ((unsigned)l0 >= (unsigned)T || (unsigned)l1 >= (unsigned)T ||
+          (unsigned)l2 >= (unsigned)T) {
+        atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);
+        continue;
+      }
+#pragma unroll
+      for (int a2 = 0; a2 < (D >= 3 ? 4 : 1); a2++)
+#pragma unroll
+        for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
+          float wy = 1.f;
+          if (D >= 2) wy *= w[1][a1];
+          if (D >= 3) wy *= w[2][a2];
+          const int rowbase = (l0) + R * ((l1 + a1) + R * (l2 + a2));
+#pragma unroll
+          for (int a0 = 0; a0 < 4; a0++) {
+            const float wt = wy * w[0][a0];
+            const int node = rowbase + a0;
+            atomicAdd(&acc[node], wt);
+#pragma unroll
+            for (int k = 0; k < D; k++) atomicAdd(&acc[(k + 1) * RD + node], wt * ys[k]);
+          }
+        }
+    }
+    __syncthreads();
+    // flush the touched region of this tile into V
+    for (int e = threadIdx.x; e < RD; e += blockDim.x) {
+      const int lx = e % R;
+      const int ly = D >= 2 ? (e / R) % R : 0;
+      const int lz = D >= 3 ? e / (R * R) : 0;
+      const int gx = o[0] + lx, gy = o[1] + ly, gz = o[2] + lz;
+      if (gx >= N || (D >= 2 && gy >= N) || (D >= 3 && gz >= N)) continue;
+      const float a0 = acc[e];
+      const float a1 = acc[RD + e];
+      const float a2 = D >= 2 ? acc[2 * RD + e] : 0.f;
+      const float a3 = D >= 3 ? acc[3 * RD + e] : 0.f;
+      if (a0 == 0.f && a1 == 0.f && a2 == 0.f && a3 == 0.f) continue;
+      long g = gx;
+      if (D >= 2) g += (long)N * gy;
+      if (D >= 3) g += (long)N * N * gz;
+      if constexpr (D == 1) {
+        atomicAdd(&V[g], make_float2(a0, a1));
+      } else {
+        atomicAdd(&V[g], make_float4(a0, a1, a2, a3));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// G2S over chunks + repulsive force numerator + Z (FP64, fixed-order finish).
+// Frep_un[i] = y_i*Phi0 - Phi_{1..d}; Z = sum_i z_i - n.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_g2s(const float4 *__restrict__ sorted, SgtState *st,
+      const int4 *__restrict__ chunks,
+      const typename Node<D>::T *__restrict__ Phi,
+      typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n) {
+  __shared__ double wz[SGT_THREADS / 32];
+  __shared__ bool last;
+  const int N = st->N, nch = st->nchunks;
+  const float maxy = st->maxy, scale = st->scale;
+  float miny[3];
+#pragma unroll
+  for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  double zacc = 0.0;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int4 ch = chunks[c];
+    for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
+      const float4 rec = sorted[j];
+      int f[3];
+      float w[3][4], ys[3];
+      sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
+      float p[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int a2 = 0; a2 < (D >= 3 ? 4 : 1); a2++)
+#pragma unroll
+        for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
+          float wy = 1.f;
+          if (D >= 2) wy *= w[1][a1];
+          if (D >= 3) wy *= w[2][a2];
+          long base = f[0];
+          if (D >= 2) base += (long)N * (f[1] + a1);
+          if (D >= 3) base += (long)N * N * (f[2] + a2);
+#pragma unroll
+          for (int a0 = 0; a0 < 4; a0++) {
+            const float wt = wy * w[0][a0];
+            const typename Node<D>::T v = __ldg(&Phi[base + a0]);
+            p[0] += wt * v.x;
+            p[1] += wt * v.y;
+            if constexpr (D >= 2) {
+              p[2] += wt * v.z;
+              if constexpr (D >= 3) p[3] += wt * v.w;
+            }
+          }
+        }
+      double ysq = 0.0, dot = 0.0;
+      typename Vec<D>::T fr;
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        ysq += (double)ys[k] * ys[k];
+        dot += (double)ys[k] * p[k + 1];
+        setcomp<D>(fr, k, ys[k] * p[0] - p[k + 1]);
+      }
+      zacc += (1.0 + 2.0 * ysq) * (double)p[0] - 2.0 * dot;
+      Frep_un[__float_as_int(rec.w)] = fr;
+    }
+  }
+  zacc = warp_sum_d(zacc);
+  if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = zacc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int k = 0; k < SGT_THREADS / 32; k++) s += wz[k];
+    part_z[blockIdx.x] = s;
+    __threadfence();
+    last = (atomicAdd(&st->done_g2s, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s = 0;
+    for (int b = 0; b < (int)gridDim.x; b++) s += __ldcg(&part_z[b]);
+    st->Z = s - (double)n;
+    st->done_g2s = 0;
+  }
+}

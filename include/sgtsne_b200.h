@@ -1,0 +1,230 @@
+/*
+ * sgtsne_b200.h -- C ABI of the B200-native SG-t-SNE gradient engine.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an sgt_status
+ * (never exits the process); sgt_last_error() explains the last failure of a
+ * context.  Device pointers must point to memory of the context's device;
+ * work is queued on the context's stream and functions that return results
+ * to the host synchronise that stream.
+ *
+ * Each declaration names the reference interface it replaces, by file:line
+ * in iakoviid/GPU-SG-SNE (CU = code/cuda/SG-tSNE-CUDA/src).
+ */
+#ifndef SGTSNE_B200_H
+#define SGTSNE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGT_ABI_VERSION 1
+
+typedef enum {
+  SGT_OK = 0,
+  SGT_ERR_INVALID_ARG = 1, /* bad size, null pointer, malformed CSR */
+  SGT_ERR_CUDA = 2,        /* a CUDA call failed */
+  SGT_ERR_NO_MEMORY = 3,   /* device or pinned allocation failed */
+  SGT_ERR_UNSUPPORTED = 4, /* option outside what the engine implements */
+  SGT_ERR_NUMERIC = 5,     /* non-finite coordinates detected */
+  SGT_ERR_NO_DEVICE = 6    /* no CUDA device */
+} sgt_status;
+
+/* Storage format of P for the attractive term: the values of the reference
+   CLI option -t (CU/testing_modules/demo_perplexity.cu:90-92) plus CSR,
+   which is the reference's format 0 (CU/pq.cu:28-30) and this engine's
+   fastest path. */
+typedef enum {
+  SGT_FORMAT_CSR = 0,
+  SGT_FORMAT_COO = 2,
+  SGT_FORMAT_HYBRID = 3 /* ELL + COO tail */
+} sgt_format;
+
+typedef enum {
+  SGT_LAYOUT_DIM_MAJOR = 0,  /* y[i + k*n]: the reference CUDA layout */
+  SGT_LAYOUT_POINT_MAJOR = 1 /* y[i*d + k]: the reference CPU layout */
+} sgt_layout;
+
+typedef enum {
+  SGT_GRID_H = 0,    /* grid follows h every iteration, mean-centred
+                        (CU/gradient_descend_varGrid.cu:68-186) */
+  SGT_GRID_FIXED = 1 /* inner grid getBestGridSize(ng)
+                        (CU/gradient_descend.cu:139-140) */
+} sgt_grid_mode;
+
+/* Parameters.  The first fourteen fields mirror tsneparams
+   (CU/types.hpp:55-72) with its meaning and defaults; the rest are
+   additions of this engine. */
+typedef struct {
+  int d;            /* embedding dimension, 1..3                       */
+  float lambda;     /* lambda rescaling target (1 = skip, as the ref.)  */
+  float alpha;      /* early exaggeration                               */
+  int max_iter;     /* iterations                                       */
+  int early_iter;   /* last iteration (inclusive) with alpha            */
+  int n;            /* number of points                                 */
+  float h;          /* grid spacing; <= 0 picks 0.5/0.7/1.2 for d=1/2/3 */
+  int drop_leaf;    /* zero the edge of single-edge rows after lambda   */
+  int np;           /* reference worker count; accepted and ignored     */
+  int format;       /* sgt_format                                       */
+  int bs;           /* reference block size; accepted and ignored       */
+  int compute_error;/* > 0: relative L2 error of F_rep every 10 iters   */
+  int ng;           /* inner grid size for SGT_GRID_FIXED (default 50)  */
+  int sim;          /* reference synthetic-data switch; ignored         */
+  /* additions */
+  int grid_mode;    /* sgt_grid_mode (default SGT_GRID_H)               */
+  int lambda_dist;  /* 1: P values are distances, 0: probabilities      */
+  int max_grid;     /* largest grid points per axis to provision
+                       (0 = 512 for d <= 2, 128 for d = 3)              */
+  int kl_every;     /* > 0: record the KL cost every kl_every iters     */
+  uint64_t seed;    /* seed of the random Y0 when y_in is NULL          */
+} sgt_params;
+
+/* Fill *p with the reference defaults (d=2, lambda=1, alpha=12,
+   max_iter=1000, early_iter=250, h=-1, format=SGT_FORMAT_COO, ng=50). */
+void sgt_params_default(sgt_params *p);
+
+typedef struct sgt_ctx sgt_ctx;
+typedef struct sgt_job sgt_job;
+
+int sgt_abi_version(void);
+const char *sgt_status_string(sgt_status s);
+
+sgt_status sgt_create(int device, sgt_ctx **out);
+void sgt_destroy(sgt_ctx *ctx);
+/* Queue all work of ctx on a caller-owned cudaStream_t (NULL = own stream). */
+sgt_status sgt_set_stream(sgt_ctx *ctx, void *cuda_stream);
+const char *sgt_last_error(const sgt_ctx *ctx);
+
+/* ---- library entry ------------------------------------------------------
+ * Replaces sgtsneCUDA<float>(P, params, y_in, timeInfo)
+ * (CU/sgtsne.cuh:21-27, CU/sgtsne.cu:25-129).
+ * P: host CSR of the kNN graph (n rows, rowptr[n+1], col/val[rowptr[n]]).
+ * As the reference: lambda rescaling unless lambda == 1, symmetrisation
+ * (P + P^T)/(2n), format preparation, max_iter iterations, final centring.
+ * y_in: host, dim-major n*d, or NULL for 1e-4 * N(0,1) from
+ * std::default_random_engine (CU/utils.cu:185-193).  y_out: host, dim-major
+ * n*d, caller-owned (the reference returned a malloc'd array).
+ * time_info: NULL or >= 7003 doubles; [7000] = total ms, [7001] = setup ms,
+ * [7002] = Z of the last iteration. */
+sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const int *col,
+                     const float *val, const sgt_params *params,
+                     const float *y_in, float *y_out, double *time_info);
+
+/* ---- device-resident job (the iteration loop of kl_minimization,
+ * CU/gradient_descend.cu:102-282, split so P and Y stay in HBM) ----------
+ * P is the already symmetric, normalised CSR (what kl_minimization gets).
+ * mem_is_device: 1 if the pointers are device pointers of ctx's device. */
+sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n,
+                          const int *rowptr, const int *col, const float *val,
+                          int mem_is_device, sgt_job **out);
+void sgt_job_destroy(sgt_job *job);
+/* Set coordinates and reset the schedule (iteration 0, uY = 0, gains = 1). */
+sgt_status sgt_job_set_y(sgt_job *job, const float *y, int layout,
+                         int mem_is_device);
+/* Queue `iters` iterations (captured CUDA graph); asynchronous. */
+sgt_status sgt_job_run(sgt_job *job, int iters);
+/* Copy the current coordinates out (synchronises).  centre = 1 subtracts the
+   mean like the reference does after the last iteration. */
+sgt_status sgt_job_get_y(sgt_job *job, float *y, int layout, int mem_is_device,
+                         int centre);
+typedef struct {
+  int iter;          /* iterations done                          */
+  int grid_points;   /* grid points per axis of the last step     */
+  float h_eff;       /* grid spacing of the last step             */
+  double zeta;       /* Z of the last step                        */
+  double kl;         /* last KL value recorded (kl_every > 0)     */
+  int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
+  long nnz;          /* nonzeros of P                             */
+} sgt_job_info;
+sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
+/* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
+sgt_status sgt_job_kl(sgt_job *job, double alpha, double *kl);
+/* Run `iters` iterations stage by stage, adding per-stage milliseconds into
+   stage_ms[8] = {bin, s2g, g2g, g2s, attractive+update, total, -, -}. */
+sgt_status sgt_job_profile(sgt_job *job, int iters, double *stage_ms);
+
+/* ---- stage operators (device pointers, queued on the context stream) --- */
+
+/* F_attr = sum_j p_ij (y_i - y_j)/(1+|y_i-y_j|^2).  Replaces
+   AttractiveEstimation (CU/pq.cu:24-57, CU/pq.cuh:8-10).
+   format CSR: rowptr/col/val; COO: rowptr = NULL, rows in `coo_rows`;
+   HYBRID: CSR input, split internally with the CUSP width rule. */
+sgt_status sgt_attractive(sgt_ctx *ctx, int format, int n, int d, long nnz,
+                          const int *rowptr, const unsigned *coo_rows,
+                          const int *col, const float *val, const float *y,
+                          int layout, float *f);
+
+/* Interpolated repulsion.  Replaces computeFrepulsive_interp
+   (CU/Frep.cu:81-125; h-driven grid as CU/Frep_varGrid.cu:79-107 and
+   CU/gradient_descend_varGrid.cu:83-92).  ng_fixed > 0 forces the inner grid
+   getBestGridSize(ng_fixed).  Outputs: f (normalised by Z, layout as y),
+   *zeta, *grid_points, *h_eff (host pointers, any may be NULL). */
+sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
+                         const float *y, int layout, float *f, double *zeta,
+                         int *grid_points, float *h_eff);
+
+/* The integer part of the repulsion: per point and dim the floor bin of the
+   scaled coordinate (CU/nuconv.cu:9-36 + CU/gridding.cu:159-167), and the
+   grid size.  bins: device uint32 n*d point-major. */
+sgt_status sgt_bins(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
+                    const float *y, int layout, uint32_t *bins,
+                    int *grid_points);
+
+/* The charge grid after S2G and the potential grid after G2G of the last
+   sgt_repulsive call: host float arrays of (d+1) * grid_points^d,
+   channel-major [c][z][y][x].  Either may be NULL. */
+sgt_status sgt_last_grids(sgt_ctx *ctx, float *v_grid, float *phi_grid);
+
+/* getBestGridSize (CU/utils.cu:194-215): smallest table size >= ng+2, minus 2. */
+int sgt_best_grid_size(int ng);
+
+/* KL cost (CU/pq.cu:61-125, tsneCost) with FP64 terms and sum. */
+sgt_status sgt_kl(sgt_ctx *ctx, int n, int d, long nnz, const int *rowptr,
+                  const int *col, const float *val, const float *y, int layout,
+                  double alpha, double zeta, double *kl);
+
+/* lambda rescaling, one warp per row, FP64 sums.  Replaces
+   lambdaRescalingGPU (CU/graph_rescaling.cu:96-107) with the semantics of
+   HYB/graph_rescaling.cpp:19-104 (dist != 0: values are distances).
+   val is rescaled in place; sigma (device, n) may be NULL. */
+sgt_status sgt_lambda_bisect(sgt_ctx *ctx, int n, const int *rowptr,
+                             float *val, float lambda, int dist, float *sigma);
+
+/* Perplexity equalisation of kNN distances.  Replaces
+   perplexityEqualization / SearchPerplexity (CU/perplexity_search.cu:113-208;
+   FP64 as HYB/sgtsne.cpp:201-254).  dist: device n*k squared distances
+   (self excluded), p: device n*k output rows summing to one, beta: device n
+   or NULL.  k <= 256. */
+sgt_status sgt_perplexity(sgt_ctx *ctx, int n, int k, const float *dist,
+                          float perplexity, float *p, float *beta);
+
+/* CSR -> COO row expansion (CU/prepareMatrix.cu:2-27); device pointers. */
+sgt_status sgt_csr_to_coo(sgt_ctx *ctx, int n, long nnz, const int *rowptr,
+                          unsigned *rows);
+
+/* ELL width by the CUSP rule used in CU/matrix_converter.cpp:236-239
+   (host rowptr). */
+int sgt_ell_width(int n, const int *rowptr);
+
+/* CSR -> ELL (column-major n*W, padding col 0 / val 0) + COO tail in row
+   order (CU/prepareMatrix.cu:55-97, CU/matrix_converter.cpp:106-207).
+   Host arrays; coo_* sized nnz.  *coo_size receives the tail length. */
+sgt_status sgt_csr_to_hybrid(int n, const int *rowptr, const int *col,
+                             const float *val, int width, unsigned *ell_cols,
+                             float *ell_vals, unsigned *coo_rows,
+                             unsigned *coo_cols, float *coo_vals,
+                             long *coo_size);
+
+/* (P + P^T) * scale with sorted columns per row (CU/graph_rescaling.cu:266-398
+   uses scale 1/(2n)).  Host arrays.  Call with out_col == NULL to get
+   *out_nnz, then again with out arrays of that size. */
+sgt_status sgt_symmetrize(int n, const int *rowptr, const int *col,
+                          const float *val, float scale, int *out_rowptr,
+                          int *out_col, float *out_val, long *out_nnz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SGTSNE_B200_H */

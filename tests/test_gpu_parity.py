@@ -1,0 +1,270 @@
+"""GPU parity tests: the CUDA engine, called through the C ABI, against the
+oracle on the same seeded inputs.
+
+Tolerances (FP32 engine vs FP64 oracle):
+  integer work (bins, grid sizes, CSR->COO, formats)      bit-exact
+  attractive forces                                       rel L2 <= 1e-5
+  S2G grid / G2G grid / repulsive forces / Z at a fixed Y rel L2 <= 1e-4
+  KL                                                      rel <= 1e-5
+  lambda / perplexity values                              rel <= 1e-4
+  iterations (same P, Y0): KL after the run               within 1 %
+"""
+import numpy as np
+import pytest
+
+from conftest import make_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import sgtsne_b200 as S
+    c = S.Context(0)
+    yield c
+    c.close()
+
+
+def dev(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+def coords(kind, n, d, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "gauss":
+        Y = rng.standard_normal((n, d)) * 5
+    elif kind == "uniform":
+        Y = rng.random((n, d))
+    elif kind == "clusters":
+        c = rng.standard_normal((8, d)) * 20
+        Y = c[rng.integers(0, 8, n)] + rng.standard_normal((n, d))
+    elif kind == "tiny":
+        Y = rng.standard_normal((n, d)) * 1e-4
+    elif kind == "offset":  # every coordinate above 100: the 100.0 min-init quirk
+        Y = 150 + rng.random((n, d)) * 30
+    else:
+        raise ValueError(kind)
+    return Y.astype(np.float32)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("kind", ["gauss", "uniform", "clusters", "tiny", "offset"])
+@pytest.mark.parametrize("ng", [0, 50])
+def test_bins_and_grid_bit_exact(torch, ctx, oracle, d, kind, ng):
+    import sgtsne_b200 as S
+    n = 20000
+    Y = coords(kind, n, d, seed=d * 7 + len(kind))
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    out = torch.empty(n * d, dtype=torch.int32, device="cuda")
+    N = ctx.bins(n, d, h, ng, dev(torch, Y), S.LAYOUT_POINT_MAJOR, out)
+    b_ref, _, _, N_ref, _ = oracle.bins_f32(Y, h, oracle.best_grid_size(ng) if ng else 0)
+    assert N == N_ref
+    assert np.array_equal(out.cpu().numpy().view(np.uint32).reshape(n, d), b_ref)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("kind", ["gauss", "clusters", "uniform"])
+def test_repulsive_vs_oracle(torch, ctx, oracle, d, kind):
+    import sgtsne_b200 as S
+    n = 8000 if d < 3 else 4000
+    Y = coords(kind, n, d, seed=11 + d)
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    Z, N, he = ctx.repulsive(n, d, h, 0, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    F = f.cpu().numpy().reshape(n, d)
+    Fo, Zo, No, heo = oracle.repulsive_interp(Y.astype(np.float64), h, n1_force=N - 2)
+    assert N == No
+    assert abs(he - heo) <= 1e-6 * heo
+    assert abs(Z - Zo) <= 1e-4 * abs(Zo)
+    assert rel(F, Fo) <= 1e-4
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_grids_vs_oracle(torch, ctx, oracle, d):
+    """S2G and G2G stage by stage: the engine's charge grid against the
+    oracle's S2G of the same FP32-scaled coordinates, and its potential grid
+    against the oracle's G2G of the engine's own charge grid."""
+    import sgtsne_b200 as S
+    n = 6000
+    Y = coords("clusters", n, d, seed=3 + d)
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    Z, N, he = ctx.repulsive(n, d, h, 0, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    V, Phi = ctx.last_grids(d, N)
+    _, sc, sh, N2, _ = oracle.bins_f32(Y, h)
+    assert N2 == N
+    q = np.concatenate([np.ones((n, 1)), sh.astype(np.float64)], 1)
+    Vo = oracle.s2g(sc.astype(np.float64), q, N)
+    assert rel(V, Vo) <= 1e-5
+    Phio = oracle.g2g(V.astype(np.float64), float(he), 1)
+    assert rel(Phi, Phio) <= 1e-4
+
+
+@pytest.mark.parametrize("fmt", [0, 2, 3])
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_attractive_formats(torch, ctx, oracle, fmt, d):
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=3000, k=12, seed=d)
+    n = len(rp) - 1
+    rng = np.random.default_rng(5)
+    Y = (rng.standard_normal((n, d)) * 3).astype(np.float32)
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    rows = dev(torch, np.repeat(np.arange(n), np.diff(rp)).astype(np.int32))
+    ctx.attractive(fmt, n, d, int(rp[-1]), dev(torch, rp), rows, dev(torch, col),
+                   dev(torch, val.astype(np.float32)), dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    Fo = oracle.attractive(rp, col, val.astype(np.float32).astype(np.float64), Y.astype(np.float64))
+    assert rel(f.cpu().numpy().reshape(n, d), Fo) <= 1e-5
+
+
+def test_dim_major_layout(torch, ctx, oracle):
+    import sgtsne_b200 as S
+    n, d = 5000, 2
+    Y = coords("gauss", n, d, 9)
+    f1 = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    f2 = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    z1, _, _ = ctx.repulsive(n, d, 0.7, 0, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f1)
+    z2, _, _ = ctx.repulsive(n, d, 0.7, 0, dev(torch, Y.T.copy()), S.LAYOUT_DIM_MAJOR, f2)
+    assert rel(f2.cpu().numpy().reshape(d, n).T, f1.cpu().numpy().reshape(n, d)) <= 1e-6
+    assert abs(z1 - z2) <= 1e-9 * abs(z1)
+
+
+def test_csr_to_coo_bit_exact(torch, ctx, oracle):
+    rp, col, val, _ = make_problem(n=2500, k=9)
+    rp2 = rp.copy()
+    n = len(rp2) - 1
+    rows = torch.empty(int(rp2[-1]), dtype=torch.int32, device="cuda")
+    ctx.csr_to_coo(n, int(rp2[-1]), dev(torch, rp2), rows)
+    assert np.array_equal(rows.cpu().numpy(), oracle.csr_to_coo(rp2))
+
+
+def test_kl(torch, ctx, oracle):
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=2000, k=10)
+    n = len(rp) - 1
+    Y = coords("gauss", n, 2, 2)
+    v32 = val.astype(np.float32)
+    kl = ctx.kl(n, 2, int(rp[-1]), dev(torch, rp), dev(torch, col), dev(torch, v32),
+                dev(torch, Y), S.LAYOUT_POINT_MAJOR, 12.0, 1234.5)
+    ko = oracle.kl(rp, col, v32.astype(np.float64), Y.astype(np.float64), 12.0, 1234.5)
+    assert abs(kl - ko) <= 1e-5 * abs(ko)
+
+
+@pytest.mark.parametrize("lam", [1.0, 10.0])
+def test_lambda_bisect(torch, ctx, oracle, lam):
+    from sgtsne_b200 import workloads as W
+    X, _ = W.gmm_isotropic(3000, 20, 5, 16.0, 6)
+    idx, d2 = W.knn_numpy(X, 20)
+    rp, col, val = W.knn_csr(idx, d2)
+    v = dev(torch, val.astype(np.float32))
+    sig = torch.empty(3000, dtype=torch.float32, device="cuda")
+    ctx.lambda_bisect(3000, dev(torch, rp), v, lam, 1, sig)
+    vo, so = oracle.lambda_rescale(rp, val.astype(np.float32).astype(np.float64), lam, dist=True)
+    assert rel(v.cpu().numpy(), vo) <= 1e-4
+    assert rel(sig.cpu().numpy(), so) <= 1e-4
+
+
+def test_perplexity(torch, ctx, oracle):
+    from sgtsne_b200 import workloads as W
+    X, _ = W.gmm_isotropic(3000, 20, 5, 16.0, 8)
+    idx, d2 = W.knn_numpy(X, 90)
+    d2 = d2 / d2.max()
+    p = torch.empty(3000 * 90, dtype=torch.float32, device="cuda")
+    ctx.perplexity(3000, 90, dev(torch, d2.astype(np.float32)), 30.0, p)
+    D = np.concatenate([np.zeros((3000, 1)), d2.astype(np.float32).astype(np.float64)], 1)
+    Po = oracle.perplexity(D, 30.0)
+    assert rel(p.cpu().numpy().reshape(3000, 90), Po) <= 1e-4
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_iterations_vs_oracle(torch, ctx, oracle, d):
+    """The graph-captured iteration loop against the oracle's gradient
+    descent (h-driven grid, per-iteration centring) on the same P and Y0."""
+    import sgtsne_b200 as S
+    rp, col, val, lab = make_problem(n=2000, k=12, seed=20 + d)
+    n = len(rp) - 1
+    rng = np.random.default_rng(1)
+    Y0 = (rng.standard_normal((n, d)) * 1e-2).astype(np.float32)
+    v32 = val.astype(np.float32)
+    p = S.default_params(d=d, format=S.FORMAT_CSR, max_iter=400, early_iter=100)
+    job = S.Job(ctx, p, rp, col, v32, device_mem=False)
+    job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+    job.run(400)
+    Y = job.get_y(np.empty((n, d), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+    info = job.info()
+    assert info.iter == 400 and info.error_flags == 0
+    Yo = oracle.kl_minimization(rp, col, v32.astype(np.float64), Y0.astype(np.float64), 400,
+                                early_iter=100, alpha=12.0, h=p.h if p.h > 0 else
+                                {1: 0.5, 2: 0.7, 3: 1.2}[d], grid_mode=0)
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    _, Zg, _, _ = oracle.repulsive_interp(Y.astype(np.float64), h)
+    _, Zo, _, _ = oracle.repulsive_interp(Yo, h)
+    klg = oracle.kl(rp, col, v32.astype(np.float64), Y.astype(np.float64), 1.0, Zg)
+    klo = oracle.kl(rp, col, v32.astype(np.float64), Yo, 1.0, Zo)
+    assert abs(klg - klo) <= 0.01 * klo
+    job.close()
+
+
+def test_formats_same_trajectory(torch, ctx):
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=3000, k=12, seed=4)
+    n = len(rp) - 1
+    Y0 = (np.random.default_rng(2).standard_normal((n, 2)) * 1e-2).astype(np.float32)
+    out = {}
+    for fmt in (0, 2, 3):
+        p = S.default_params(d=2, format=fmt)
+        job = S.Job(ctx, p, rp, col, val.astype(np.float32), device_mem=False)
+        job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+        job.run(30)
+        out[fmt] = job.get_y(np.empty((n, 2), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        job.close()
+    assert rel(out[2], out[0]) <= 1e-3
+    assert rel(out[3], out[0]) <= 1e-3
+
+
+def test_embed_dropin(torch, ctx, oracle):
+    """sgt_embed (the sgtsneCUDA flow: lambda rescaling, symmetrisation,
+    iterations, centring) against the oracle pipeline."""
+    import sgtsne_b200 as S
+    from sgtsne_b200 import workloads as W
+    n, k = 2500, 15
+    X, _ = W.gmm_isotropic(n, 20, 6, 16.0, 12)
+    idx, d2 = W.knn_numpy(X, k)
+    rp, col, val = W.knn_csr(idx, d2)
+    val = (val / val.max()).astype(np.float32)
+    Y0 = (np.random.default_rng(3).standard_normal((n, 2)) * 1e-2).astype(np.float32)
+    p = S.default_params(d=2, lambda_=1.0, max_iter=300, early_iter=100, format=S.FORMAT_CSR)
+    p.lambda_ = 10.0
+    Y, ti = ctx.embed(rp, col, val, p, y_in=Y0.T.copy())
+    assert np.abs(Y.mean(0)).max() < 1e-3
+    vo, _ = oracle.lambda_rescale(rp, val.astype(np.float64), 10.0, dist=True)
+    srp, sc, sv = oracle.symmetrize(rp, col, vo, 1.0 / (2 * n))
+    Yo = oracle.kl_minimization(srp, sc, sv, Y0.astype(np.float64), 300, early_iter=100,
+                                alpha=12.0, h=0.7, grid_mode=0)
+    _, Zg, _, _ = oracle.repulsive_interp(Y.astype(np.float64), 0.7)
+    _, Zo, _, _ = oracle.repulsive_interp(Yo, 0.7)
+    klg = oracle.kl(srp, sc, sv, Y.astype(np.float64), 1.0, Zg)
+    klo = oracle.kl(srp, sc, sv, Yo, 1.0, Zo)
+    assert abs(klg - klo) <= 0.01 * klo
+    assert ti[7000] > 0
+
+
+def test_invalid_csr_rejected(torch, ctx):
+    import sgtsne_b200 as S
+    rp = np.array([0, 2, 1, 3], np.int32)  # not monotone
+    col = np.array([1, 2, 0], np.int32)
+    p = S.default_params(d=2, format=S.FORMAT_CSR)
+    with pytest.raises(S.SgtError) as e:
+        S.Job(ctx, p, rp, col, np.ones(3, np.float32), device_mem=False)
+    assert e.value.status == 1
