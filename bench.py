@@ -1,0 +1,415 @@
+"""Benchmark: SG-t-SNE gradient iterations per second on one embedding of
+n = 1.3M points in 2-D (the 1.3M-point configuration: 50-D 40-component
+Zipf(1.1) Gaussian mixture, exact kNN k = 30, lambda = 10, symmetrised,
+h = 0.7, cubic interpolation).
+
+A step is one full gradient iteration (attractive SpMV, FFT-interpolated
+repulsion, Z, gains/momentum update).  Steps start from a fixed expanded
+embedding (a random 2-D projection of the data scaled so the grid is at its
+largest size, 512 points per axis: the late-run regime), after W untimed
+warm-up steps.  P (>= 400 MB) and the per-point arrays exceed the 126 MB L2,
+so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  Each rank runs an independent
+replica of the embedding (the single-embedding path is not sharded: replicas
+only); value = N * K / max-over-ranks time.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "gpu-sg-sne_b200", "python"))
+sys.path.insert(0, REPO)
+
+METRIC = "t-SNE iters/s at n=1.3M,d=2 (%HBM roofline); served embeds/s, p99 vs plain"
+PUBLISHED_ITERS_PER_S = 4.4  # 1.3M points, d=2, GTX 1060 (README chart, ~225 s / 1000 it)
+WORKLOAD = ("n=1,300,000 FP32 points in 50-D, 40-component Gaussian mixture with "
+            "Zipf(1.1) sizes, centres N(0,25I), eigenvalues U(0.2,2) under random rotations; "
+            "exact kNN k=30, lambda=10 bisection on squared distances, (P+P^T)/(2n); "
+            "d=2, h=0.7, cubic Lagrange (np=3)")
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (also exercised by tests/test_bench_dist.py on gloo)
+# ---------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def dist_init(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None:
+            dist.barrier(device_ids=[device])
+        else:
+            dist.barrier()
+
+
+def max_over_ranks(dist, value, device="cpu"):
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def build_knn(n, seed, device):
+    from sgtsne_b200 import workloads as W
+    X, _ = W.gmm_zipf(n, dim=50, ncomp=40, zipf_a=1.1, centre_var=25.0, seed=seed)
+    idx, d2 = W.knn_torch(X, 30, device=device, block=1024)
+    if str(device).startswith("cuda"):
+        import torch
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return X, idx, d2
+
+
+def expanded_state(X, d, spread, seed):
+    """Fixed expanded embedding: random 2-D projection of X, per-axis std =
+    spread (the late-run regime of the iteration)."""
+    rng = np.random.default_rng(seed + 1)
+    R = rng.standard_normal((X.shape[1], d)).astype(np.float32)
+    Y = X @ R
+    Y = (Y - Y.mean(0)) / Y.std(0) * spread
+    return np.ascontiguousarray(Y.astype(np.float32))
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(nnz, n):
+    """Per-launch DRAM bytes of the fused row kernel from the committed ncu
+    summary, scaled from its capture size to this launch (traffic grows with
+    nnz and n)."""
+    path = os.path.join(REPO, "profiles", "row_update_traffic.txt")
+    try:
+        kv = {}
+        for line in open(path):
+            if ":" in line:
+                k, v = line.split(":", 1)
+                kv[k.strip()] = v.strip()
+        b = float(kv["dram_bytes_per_launch"])
+        alg = float(kv["algorithmic_bytes_per_launch"])
+        return b / alg  # ratio applied to this launch's algorithmic bytes
+    except Exception:
+        return None
+
+
+def row_alg_bytes(n, nnz, d):
+    """Algorithmic bytes of one fused row launch: P stream (8 B/nnz + rowptr),
+    Y read once, F_rep numerator read, uY/gains read+write, Ynext write."""
+    S = 4 if d == 3 else d
+    return 8 * nnz + 4 * (n + 1) + 4 * n * S * (1 + 1 + 2 + 2 + 1)
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local, dist):
+    import torch
+
+    import sgtsne_b200 as S
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    n, d = args.n, 2
+    t_setup = time.time()
+    X, idx, d2 = build_knn(n, args.seed, dev)
+    ctx = S.Context(local)
+    # one non-default stream for the engine and the timing events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    k = idx.shape[1]
+    rp_knn = torch.arange(0, (n + 1) * k, k, dtype=torch.int32, device=dev)
+    vals = d2.reshape(-1).contiguous().clone()
+    ctx.lambda_bisect(n, rp_knn, vals, 10.0, 1)
+    rp_h = rp_knn.cpu().numpy()
+    col_h = idx.reshape(-1).cpu().numpy().astype(np.int32)
+    val_h = vals.cpu().numpy()
+    srp, sc, sv = S.symmetrize(rp_h, col_h, val_h, 1.0 / (2 * n))
+    nnz = int(srp[-1])
+    t_setup = time.time() - t_setup
+    p = S.default_params(d=d, format=S.FORMAT_CSR, max_iter=1000, early_iter=250, h=0.7)
+    p.lambda_ = 10.0
+    Ystate = expanded_state(X, d, args.spread, args.seed)
+    del X
+
+    # ---- value: device-resident inputs ----
+    job = S.Job(ctx, p, torch.from_numpy(srp).to(dev), torch.from_numpy(sc).to(dev),
+                torch.from_numpy(sv).to(dev), device_mem=True)
+    Yd = torch.from_numpy(Ystate).to(dev)
+    job.set_y(Yd, S.LAYOUT_POINT_MAJOR, True)
+    job.run(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    job.run(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(dist, local)
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
+    info = job.info()
+    # per-kernel durations on the same stream (same kernels, bracketed)
+    stage = job.profile(args.steps)
+    row_ms = stage[4] / args.steps
+    stage_avg = (stage[:6] / args.steps).tolist()
+    job.close()
+
+    # ---- e2e: through the C ABI from pinned host buffers ----
+    rp_pin = torch.from_numpy(srp).pin_memory()
+    c_pin = torch.from_numpy(sc).pin_memory()
+    v_pin = torch.from_numpy(sv).pin_memory()
+    y_pin = torch.from_numpy(Ystate).pin_memory()
+    y_out = torch.empty_like(y_pin).pin_memory()
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    job2 = S.Job(ctx, p, rp_pin, c_pin, v_pin, device_mem=False)
+    job2.set_y(y_pin, S.LAYOUT_POINT_MAJOR, False)
+    job2.run(args.steps)
+    job2.get_y(y_out, S.LAYOUT_POINT_MAJOR, False, 1)
+    t1 = time.perf_counter()
+    barrier(dist, local)
+    e2e_s = max_over_ranks(dist, t1 - t0, dev)
+    job2.close()
+    h2d = (srp.nbytes + sc.nbytes + sv.nbytes + Ystate.nbytes) / args.steps
+    d2h = Ystate.nbytes / args.steps
+
+    # ---- full run from Y0 (whole 1000-iteration job, extra information) ----
+    full = None
+    if args.full_run:
+        job3 = S.Job(ctx, p, torch.from_numpy(srp).to(dev), torch.from_numpy(sc).to(dev),
+                     torch.from_numpy(sv).to(dev), device_mem=True)
+        y0 = torch.randn(n, d, device=dev, generator=torch.Generator(dev).manual_seed(0)) * 1e-2
+        job3.set_y(y0.contiguous(), S.LAYOUT_POINT_MAJOR, True)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        job3.run(1000)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        full = {"iters": 1000, "ms": f0.elapsed_time(f1),
+                "iters_per_s": 1000.0 / (f0.elapsed_time(f1) / 1e3),
+                "final_grid_points": job3.info().grid_points}
+        job3.close()
+
+    out = None
+    if rank == 0:
+        alg = row_alg_bytes(n, nnz, d)
+        hbm, src = peaks()
+        achieved = alg / (row_ms / 1e3) / 1e9
+        ratio = read_traffic(nnz, n)
+        per_iter_kernels = 10  # bin x3, s2g, fft x3, g2s, row, stats
+        out = {
+            "metric": METRIC, "value": world * args.steps / (ms / 1e3), "unit": "iters/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": (world * args.steps / (ms / 1e3)) / PUBLISHED_ITERS_PER_S,
+            "dtype": "f32 (FP64 Z/KL/row-sum reductions)",
+            "data": "synthetic (seeded generator with the configuration's shapes)",
+            "config": {"workload": WORKLOAD, "n": n, "d": d, "nnz": nnz, "format": "csr",
+                       "parallelism": f"replicas x{world}", "grid_points": info.grid_points,
+                       "h_eff": round(info.h_eff, 5), "row_group": info.row_group,
+                       "row_group_tune_ms": [round(x, 4) for x in info.tune_ms],
+                       "timed_state":
+                       f"fixed expanded embedding (std {args.spread}), {args.warmup} warm-up steps",
+                       "l2": "inputs larger than L2 (P >= 400 MB), no flush",
+                       "stage_ms": dict(zip(["bin", "s2g", "g2g", "g2s", "attr+update",
+                                             "total"], [round(x, 4) for x in stage_avg])),
+                       "setup_s": round(t_setup, 1), "full_run": full},
+            "roofline": {"bound": "hbm", "kernel": "k_row_update (fused CSR SpMV + update)",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_source": src,
+                         "algorithmic_bytes_per_launch": alg,
+                         "traffic": None if ratio is None else ratio * alg},
+            "e2e": {"value": world * args.steps / e2e_s, "unit": "iters/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "includes": "job create from pinned host CSR, H2D, K iterations, D2H of Y"},
+            "gpu_launches": per_iter_kernels * args.steps,
+            "clocks": clk,
+        }
+    ctx.close()
+    return out, (srp, sc, sv, Ystate)
+
+
+def cpu_sample(srp, sc, sv, Ystate, iters, threads):
+    """The oracle (FP64 CPU path: CSR SpMV, FFT repulsion, update) on the
+    same P and state; returns seconds per iteration."""
+    from oracle import oracle as O
+    Y = Ystate.astype(np.float64)
+    t = time.perf_counter()
+    O.kl_minimization(srp, sc, sv.astype(np.float64), Y, iters, early_iter=250, alpha=12.0,
+                      h=0.7, grid_mode=0, nthreads=threads)
+    return (time.perf_counter() - t) / iters
+
+
+def run_reference(args, rank, world, local, dist):
+    """The reference's CPU path, restated by the oracle (the reference's own
+    CPU code needs Cilk Plus and FFTW, absent here), with all host threads."""
+    if rank != 0:
+        return None
+    import torch
+    from oracle import oracle as O
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    n = args.n
+    X, idx, d2 = build_knn(n, args.seed, dev)
+    k = idx.shape[1]
+    rp = (np.arange(n + 1, dtype=np.int64) * k).astype(np.int32)
+    col = idx.reshape(-1).cpu().numpy().astype(np.int32)
+    val = d2.reshape(-1).cpu().numpy().astype(np.float64)
+    v, _ = O.lambda_rescale(rp, val, 10.0, dist=True)
+    srp, sc, sv = O.symmetrize(rp, col, v, 1.0 / (2 * n))
+    Ystate = expanded_state(X, 2, args.spread, args.seed)
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, args.ref_steps))
+    cpu_sample(srp, sc, sv.astype(np.float32), Ystate, max(0, min(args.warmup, 1)), threads) \
+        if min(args.warmup, 1) > 0 else None
+    spi = cpu_sample(srp, sc, sv.astype(np.float32), Ystate, steps, threads)
+    val_ = 1.0 / spi
+    return {
+        "metric": METRIC, "impl": "reference", "value": val_, "unit": "iters/s", "n_gpus": world,
+        "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": spi * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": val_ / PUBLISHED_ITERS_PER_S,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "d": 2, "nnz": int(srp[-1]),
+                   "timed_state": f"fixed expanded embedding (std {args.spread})"},
+        "cpu_baseline": {"value": val_, "unit": "iters/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full iterations at n={n} from the expanded state"},
+        "e2e": {"value": val_, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1300000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--spread", type=float, default=60.0)
+    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--no-full-run", dest="full_run", action="store_false")
+    ap.add_argument("--no-cpu", dest="cpu", action="store_false")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    import torch
+    dist = dist_init(world, "nccl" if torch.cuda.is_available() else "gloo")
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, rank, world, local, dist)
+        else:
+            out, prob = run_ours(args, rank, world, local, dist)
+            if rank == 0 and world == 1 and args.cpu and out is not None:
+                srp, sc, sv, Ystate = prob
+                threads = os.cpu_count() or 1
+                spi = cpu_sample(srp, sc, sv, Ystate, args.cpu_iters, threads)
+                out["cpu_baseline"] = {"value": 1.0 / spi, "unit": "iters/s", "cores": threads,
+                                       "kind": "port",
+                                       "sample": f"{args.cpu_iters} full iterations at n={args.n} "
+                                                 "from the same expanded state, FP64 oracle"}
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -48,6 +48,7 @@ struct sgt_job {
   unsigned *ell_cols = nullptr;
   float *ell_vals = nullptr;
   int ell_w = 0;
+  int *perm = nullptr;  // engine slot -> caller's point index (nullptr: identity)
   float *Y = nullptr, *Ynext = nullptr, *uY = nullptr, *gains = nullptr,
         *Frep = nullptr, *Fattr = nullptr;
   float4 *sorted = nullptr;
@@ -65,6 +66,7 @@ struct sgt_job {
   cudaGraphExec_t gexec = nullptr;
   std::vector<void *> allocs;
   double last_kl = 0.0;
+  float tune_ms[4] = {0, 0, 0, 0};  // row kernel ms for G = 4, 8, 16, 32
 };
 
 // ---------------------------------------------------------------------------
@@ -272,6 +274,8 @@ static sgt_status job_shapes(sgt_job *J) {
   }
   J->nb_row = grid_blocks(nsm, occ);
   J->nb_part = std::max(std::max(J->nb_pts, J->nb_row), std::max(J->nb_g2s, J->nb_s2g));
+  // the fused CSR row kernel launches ceil(n * G / 256) blocks, G <= 32
+  J->nb_part = std::max(J->nb_part, (int)(((long)J->n * 32 + SGT_THREADS - 1) / SGT_THREADS));
   return SGT_OK;
 }
 
@@ -404,9 +408,12 @@ static sgt_status enqueue_update(sgt_job *J, cudaStream_t s) {
   typedef typename Vec<D>::T VT;
   const int n = J->n;
   if (J->format == SGT_FORMAT_CSR) {
-    k_row_update<D, G, true><<<J->nb_row, SGT_THREADS, 0, s>>>(
-        J->rowptr, J->pairs, nullptr, (const VT *)J->Y, (const VT *)J->Frep, (VT *)J->uY,
-        (VT *)J->gains, (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max, J->part_sum);
+    const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
+    k_row_fused<D, G><<<nb, SGT_THREADS, 0, s>>>(
+        J->rowptr, J->pairs, (const VT *)J->Y, (const VT *)J->Frep, (VT *)J->uY, (VT *)J->gains,
+        (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max, J->part_sum);
+    k_iter_stats<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, J->st, J->jp,
+                                                      J->part_min, J->part_max, J->part_sum);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals,
@@ -506,11 +513,13 @@ __global__ void k_write_bins(const typename Vec<D>::T *__restrict__ Y, int n,
 // mean of the current coordinates subtracted on the way out
 template <int D>
 __global__ void k_unpack_centred(const typename Vec<D>::T *__restrict__ src, int n, int dim_major,
-                                 const SgtState *st, int use_next_mean, float *__restrict__ dst) {
+                                 const SgtState *st, int use_next_mean, const int *perm,
+                                 float *__restrict__ dst) {
   float mean[3];
   for (int k = 0; k < D; k++) mean[k] = use_next_mean ? (float)(st->sum[k] / (double)n) : 0.f;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const typename Vec<D>::T v = src[i];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const typename Vec<D>::T v = src[r];
+    const int i = perm ? perm[r] : r;
 #pragma unroll
     for (int k = 0; k < D; k++) {
       const float x = comp<D>(v, k) - mean[k];
@@ -539,6 +548,82 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
   J->jp.n1_fixed = sgt_best_grid_size(ng > 0 ? ng : 50);
   J->jp.h = h > 0 ? h : (d == 1 ? 0.5f : (d == 2 ? 0.7f : 1.2f));
   return SGT_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// autotuner: lanes per row of the fused row kernel, timed on this job's P
+// (scratch copies of every array the kernel writes; the job's state is not
+// touched).  The fastest of G = 4, 8, 16, 32 is kept.
+// ---------------------------------------------------------------------------
+template <int D, int G>
+static float time_row_kernel(sgt_job *J, float *tY, float *tU, float *tG, float *tYn,
+                             SgtState *tst, cudaEvent_t e0, cudaEvent_t e1) {
+  typedef typename Vec<D>::T VT;
+  cudaStream_t s = J->ctx->stream;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0, s);
+    const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
+    k_row_fused<D, G><<<nb, SGT_THREADS, 0, s>>>(
+        J->rowptr, J->pairs, (const VT *)tY, (const VT *)J->Frep, (VT *)tU, (VT *)tG, (VT *)tYn,
+        tst, J->jp, J->part_min, J->part_max, J->part_sum);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  return best;
+}
+
+template <int D>
+static sgt_status tune_group_d(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  const size_t np = (size_t)J->n * J->S;
+  float *buf = nullptr;
+  SgtState *tst = nullptr;
+  CK(cudaMalloc(&buf, sizeof(float) * np * 4));
+  CK(cudaMalloc(&tst, sizeof(SgtState)));
+  CK(cudaMemsetAsync(buf, 0, sizeof(float) * np * 4, s));
+  CK(cudaMemsetAsync(J->Frep, 0, sizeof(float) * np, s));
+  SgtState h;
+  memset(&h, 0, sizeof(h));
+  h.Z = 1.0;
+  h.N = 16; h.M = 32; h.logM = 5; h.maxy = 1.f; h.scale = 13.f; h.T = 32; h.tiles_dim = 1; h.ntiles = 1;
+  CK(cudaMemcpyAsync(tst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float *tY = buf, *tU = buf + np, *tG = buf + 2 * np, *tYn = buf + 3 * np;
+  const int cand[4] = {4, 8, 16, 32};
+  float t[4];
+  t[0] = time_row_kernel<D, 4>(J, tY, tU, tG, tYn, tst, e0, e1);
+  t[1] = time_row_kernel<D, 8>(J, tY, tU, tG, tYn, tst, e0, e1);
+  t[2] = time_row_kernel<D, 16>(J, tY, tU, tG, tYn, tst, e0, e1);
+  t[3] = time_row_kernel<D, 32>(J, tY, tU, tG, tYn, tst, e0, e1);
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  cudaFree(tst);
+  CK(e);
+  CK(cudaGetLastError());
+  int best = 0;
+  for (int k = 1; k < 4; k++)
+    if (t[k] < t[best]) best = k;
+  J->G = cand[best];
+  for (int k = 0; k < 4; k++) J->tune_ms[k] = t[k];
+  return SGT_OK;
+}
+
+static sgt_status tune_group(sgt_job *J) {
+  switch (J->d) {
+    case 1: return tune_group_d<1>(J);
+    case 2: return tune_group_d<2>(J);
+    default: return tune_group_d<3>(J);
+  }
 }
 
 extern "C" {
@@ -626,8 +711,9 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   st = jalloc(J, &J->rowptr, (size_t)n + 1);
   if (st != SGT_OK) return bail(st);
   if (J->format == SGT_FORMAT_CSR) {
-    st = jalloc(J, &J->pairs, (size_t)nnz);
-    if (st != SGT_OK) return bail(st);
+    // 8 pairs of zero padding: the stream kernel reads whole 4-pair groups
+    if ((st = jalloc(J, &J->pairs, (size_t)nnz + 8)) != SGT_OK) return bail(st);
+    cudaMemsetAsync(J->pairs + nnz, 0, 8 * sizeof(int2), s);
   }
   const cudaMemcpyKind kind = mem_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   if (cudaMemcpyAsync(J->rowptr, rowptr, sizeof(int) * (n + 1), kind, s) != cudaSuccess)
@@ -690,6 +776,10 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   if (J->format != SGT_FORMAT_CSR) {
     if ((st = jalloc(J, &J->Fattr, (size_t)n * J->S)) != SGT_OK) return bail(st);
   }
+  if (J->format == SGT_FORMAT_CSR) {
+    st = tune_group(J);
+    if (st != SGT_OK) return bail(st);
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "job setup"));
   *out = J;
   return SGT_OK;
@@ -717,7 +807,19 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
     CK(cudaMemcpyAsync(staging, y, bytes, cudaMemcpyHostToDevice, s));
     src = staging;
   }
-  CKS(pack_y(J, src, layout, J->Ynext, s));
+  if (J->perm) {
+    // caller order -> engine order through a scratch array (Frep is free here)
+    CKS(pack_y(J, src, layout, J->Frep, s));
+    const int nb = grid_blocks(ctx->nsm, 4);
+    switch (J->d) {
+      case 1: k_permute_vec<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J->Frep, J->perm, J->n, (float *)J->Ynext); break;
+      case 2: k_permute_vec<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J->Frep, J->perm, J->n, (float2 *)J->Ynext); break;
+      default: k_permute_vec<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)J->Frep, J->perm, J->n, (float4 *)J->Ynext); break;
+    }
+    CK(cudaGetLastError());
+  } else {
+    CKS(pack_y(J, src, layout, J->Ynext, s));
+  }
   CK(cudaMemsetAsync(J->uY, 0, sizeof(float) * (size_t)J->n * J->S, s));
   {
     std::vector<float> ones((size_t)J->n * J->S, 1.0f);
@@ -780,9 +882,9 @@ sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, in
   const int nb = grid_blocks(ctx->nsm, 4);
   const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
   switch (J->d) {
-    case 1: k_unpack_centred<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J->Ynext, J->n, dm, J->st, centre, dst); break;
-    case 2: k_unpack_centred<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J->Ynext, J->n, dm, J->st, centre, dst); break;
-    default: k_unpack_centred<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)J->Ynext, J->n, dm, J->st, centre, dst); break;
+    case 1: k_unpack_centred<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J->Ynext, J->n, dm, J->st, centre, J->perm, dst); break;
+    case 2: k_unpack_centred<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J->Ynext, J->n, dm, J->st, centre, J->perm, dst); break;
+    default: k_unpack_centred<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)J->Ynext, J->n, dm, J->st, centre, J->perm, dst); break;
   }
   CK(cudaGetLastError());
   if (staging) {
@@ -808,16 +910,12 @@ sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
   info->kl = J->last_kl;
   info->error_flags = J->st_host->error;
   info->nnz = J->nnz;
+  info->row_group = J->G;
+  for (int k = 0; k < 4; k++) info->tune_ms[k] = J->tune_ms[k];
   return SGT_OK;
 }
 
 }  // extern "C"
-
-template <int D, int G>
-static void launch_kl(sgt_job *J, double alpha, cudaStream_t s) {
-  k_kl<D, G><<<J->nb_row, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const typename Vec<D>::T *)J->Y,
-                                               J->st, alpha, J->part_kl, J->n);
-}
 
 extern "C" {
 
@@ -835,7 +933,7 @@ sgt_status sgt_job_kl(sgt_job *J, double alpha, double *kl) {
     alpha = J->st_host->alpha > 0 ? J->st_host->alpha : J->p.alpha;
   }
   switch (J->d * 100 + J->G) {
-#define KLC(DD, GG) case DD * 100 + GG: launch_kl<DD, GG>(J, alpha, s); break;
+#define KLC(DD, GG) case DD * 100 + GG: k_kl<DD, GG><<<J->nb_row, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const typename Vec<DD>::T *)J->Y, J->st, alpha, J->part_kl, J->n); break;
     KLC(1, 4) KLC(1, 8) KLC(1, 16) KLC(1, 32)
     KLC(2, 4) KLC(2, 8) KLC(2, 16) KLC(2, 32)
     KLC(3, 4) KLC(3, 8) KLC(3, 16) KLC(3, 32)

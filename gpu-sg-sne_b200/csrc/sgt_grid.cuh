@@ -366,6 +366,10 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
   extern __shared__ float acc[];  // [D+1][R^D]
   const int T = st->T, td = st->tiles_dim, N = st->N, nch = st->nchunks;
   const float maxy = st->maxy, scale = st->scale;
+  // charges are taken about the middle of the grid: F and Z are invariant to
+  // the origin of y, and |y - c| <= maxy/2 halves the cancellation in
+  // (1 + 2|y|^2) Phi0 - 2 y.Phi
+  const float hc = 0.5f * maxy;
   float miny[3];
 #pragma unroll
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
@@ -411,7 +415,7 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
             const int node = rowbase + a0;
             atomicAdd(&acc[node], wt);
 #pragma unroll
-            for (int k = 0; k < D; k++) atomicAdd(&acc[(k + 1) * RD + node], wt * ys[k]);
+            for (int k = 0; k < D; k++) atomicAdd(&acc[(k + 1) * RD + node], wt * (ys[k] - hc));
           }
         }
     }
@@ -455,6 +459,7 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
   __shared__ bool last;
   const int N = st->N, nch = st->nchunks;
   const float maxy = st->maxy, scale = st->scale;
+  const float hc = 0.5f * maxy;  // charge origin used by S2G
   float miny[3];
 #pragma unroll
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
@@ -493,9 +498,10 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
       typename Vec<D>::T fr;
 #pragma unroll
       for (int k = 0; k < D; k++) {
-        ysq += (double)ys[k] * ys[k];
-        dot += (double)ys[k] * p[k + 1];
-        setcomp<D>(fr, k, ys[k] * p[0] - p[k + 1]);
+        const float yk = ys[k] - hc;
+        ysq += (double)yk * yk;
+        dot += (double)yk * p[k + 1];
+        setcomp<D>(fr, k, yk * p[0] - p[k + 1]);
       }
       zacc += (1.0 + 2.0 * ysq) * (double)p[0] - 2.0 * dot;
       Frep_un[__float_as_int(rec.w)] = fr;
@@ -512,11 +518,19 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
     last = (atomicAdd(&st->done_g2s, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
+  if (last) {
     __threadfence();
     double s = 0;
-    for (int b = 0; b < (int)gridDim.x; b++) s += __ldcg(&part_z[b]);
-    st->Z = s - (double)n;
-    st->done_g2s = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(&part_z[b]);
+    s = warp_sum_d(s);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0;
+      for (int k = 0; k < SGT_THREADS / 32; k++) t += wz[k];
+      st->Z = t - (double)n;
+      st->done_g2s = 0;
+    }
   }
 }

@@ -45,11 +45,24 @@ __device__ __forceinline__ void csr_row_sum(const int *__restrict__ rowptr,
                                             int i, int lane,
                                             const typename Vec<D>::T &yi,
                                             float *acc) {
-  const int s = __ldg(&rowptr[i]), e = __ldg(&rowptr[i + 1]);
-  for (int t = s + lane; t < e; t += G) {
-    const int2 pr = __ldg(&pairs[t]);
-    const typename Vec<D>::T yj = __ldg(&Y[pr.x]);
-    attr_term<D>(yi, yj, __int_as_float(pr.y), acc);
+  // P is streamed once per iteration: evict-first loads keep the gathered
+  // coordinates resident in L2.  Four independent (column, value) loads and
+  // four independent gathers per lane are in flight per step; a lane past
+  // the row end gathers its own point with weight 0.
+  const int s = __ldcs(&rowptr[i]), e = __ldcs(&rowptr[i + 1]);
+  constexpr int U = 4;
+  for (int t0 = s + lane; t0 < e; t0 += U * G) {
+    int2 pr[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * G;
+      pr[u] = t < e ? __ldcs(&pairs[t]) : make_int2(i, 0);
+    }
+    typename Vec<D>::T yj[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) yj[u] = __ldg(&Y[pr[u].x]);
+#pragma unroll
+    for (int u = 0; u < U; u++) attr_term<D>(yi, yj[u], __int_as_float(pr[u].y), acc);
   }
 }
 
@@ -66,77 +79,17 @@ __device__ __forceinline__ float sgn_f(float x) {
   return x == 0.f ? 0.f : (x < 0.f ? -1.f : 1.f);
 }
 
-// ---------------------------------------------------------------------------
-// Fused iteration row kernel.  FUSED: compute F_attr from CSR; otherwise read
-// it from Fattr (COO / ELL formats).  Writes Ynext, uY, gains; the last CTA
-// turns the per-block min/max/sum of Ynext into the next grid decision.
-// ---------------------------------------------------------------------------
-template <int D, int G, bool FUSED>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
-             const typename Vec<D>::T *__restrict__ Fattr,
-             const typename Vec<D>::T *__restrict__ Y,
-             const typename Vec<D>::T *__restrict__ Frep_un,
-             typename Vec<D>::T *__restrict__ uY,
-             typename Vec<D>::T *__restrict__ gains,
-             typename Vec<D>::T *__restrict__ Ynext, SgtState *st,
-             SgtJobParams jp, float4 *part_min, float4 *part_max,
-             double *part_sum) {
+// Per-block min/max/sum of Ynext -> partials; the last block reduces all
+// partials with every thread and turns them into the next grid decision.
+template <int D>
+__device__ __forceinline__ void block_finish_stats(SgtState *st, const SgtJobParams &jp,
+                                                   float *mn, float *mx, double *sm,
+                                                   float4 *part_min, float4 *part_max,
+                                                   double *part_sum, int iter, float alpha,
+                                                   float mom) {
   __shared__ float smin[SGT_THREADS / 32][3], smax[SGT_THREADS / 32][3];
   __shared__ double ssum[SGT_THREADS / 32][3];
   __shared__ bool last;
-  const int n = jp.n;
-  const int iter = st->iter;
-  const float alpha = iter <= jp.early_iter ? jp.alpha0 : 1.0f;
-  const float mom = iter <= jp.mom_switch ? 0.5f : 0.8f;
-  const float eta = jp.eta;
-  const float Zf = (float)st->Z;
-  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  double sm[3] = {0, 0, 0};
-  const int lane = threadIdx.x % G;
-  const int grp = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const int ngrp = gridDim.x * blockDim.x / G;
-  // uniform trip count per warp so the group shuffles stay converged
-  const int rounds = (n + ngrp - 1) / ngrp;
-  for (int r = 0; r < rounds; r++) {
-    const int i = grp + r * ngrp;
-    const bool valid = i < n;
-    float acc[3] = {0.f, 0.f, 0.f};
-    typename Vec<D>::T yi;
-    if (valid) yi = Y[i];
-    if (FUSED) {
-      if (valid) csr_row_sum<D, G>(rowptr, pairs, Y, i, lane, yi, acc);
-      group_reduce<D, G>(acc);
-    } else if (valid) {
-      const typename Vec<D>::T fa = Fattr[i];
-#pragma unroll
-      for (int k = 0; k < D; k++) acc[k] = comp<D>(fa, k);
-    }
-    if (valid && lane == 0) {
-      const typename Vec<D>::T fr = Frep_un[i];
-      typename Vec<D>::T u = uY[i], g = gains[i], yn = yi;
-#pragma unroll
-      for (int k = 0; k < D; k++) {
-        const float frep = comp<D>(fr, k) / Zf;
-        const float dy = alpha * acc[k] - frep;
-        float gk = comp<D>(g, k), uk = comp<D>(u, k);
-        gk = (sgn_f(dy) != sgn_f(uk)) ? (float)((double)gk + 0.2) : (float)((double)gk * 0.8);
-        if ((double)gk < 0.01) gk = (float)0.01;
-        uk = mom * uk - eta * gk * dy;
-        const float y = comp<D>(yi, k) + uk;
-        setcomp<D>(g, k, gk);
-        setcomp<D>(u, k, uk);
-        setcomp<D>(yn, k, y);
-        mn[k] = fminf(mn[k], y);
-        mx[k] = fmaxf(mx[k], y);
-        sm[k] += (double)y;
-      }
-      if constexpr (D == 3) { u.w = 0.f; g.w = 0.f; yn.w = 0.f; }
-      uY[i] = u;
-      gains[i] = g;
-      Ynext[i] = yn;
-    }
-  }
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < D; k++) {
@@ -161,18 +114,36 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
     last = (atomicAdd(&st->done_row, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    double s[3] = {0, 0, 0};
-    for (int b = 0; b < (int)gridDim.x; b++) {
-      lo[0] = fminf(lo[0], __ldcg(&part_min[b].x));
-      hi[0] = fmaxf(hi[0], __ldcg(&part_max[b].x));
-      if (D > 1) { lo[1] = fminf(lo[1], __ldcg(&part_min[b].y)); hi[1] = fmaxf(hi[1], __ldcg(&part_max[b].y)); }
-      if (D > 2) { lo[2] = fminf(lo[2], __ldcg(&part_min[b].z)); hi[2] = fmaxf(hi[2], __ldcg(&part_max[b].z)); }
-      for (int k = 0; k < D; k++) s[k] += __ldcg(&part_sum[b * 4 + k]);
-    }
+  if (!last) return;
+  __threadfence();
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double s[3] = {0, 0, 0};
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    const float4 a = __ldcg(&part_min[b]), c = __ldcg(&part_max[b]);
+    lo[0] = fminf(lo[0], a.x); hi[0] = fmaxf(hi[0], c.x);
+    lo[1] = fminf(lo[1], a.y); hi[1] = fmaxf(hi[1], c.y);
+    lo[2] = fminf(lo[2], a.z); hi[2] = fmaxf(hi[2], c.z);
+    for (int k = 0; k < D; k++) s[k] += __ldcg(&part_sum[b * 4 + k]);
+  }
+  // fixed-order tree: warp shuffles then warp 0 over the warp results
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    lo[k] = warp_min_f(lo[k]);
+    hi[k] = warp_max_f(hi[k]);
+    s[k] = warp_sum_d(s[k]);
+  }
+  __syncthreads();
+  if (l == 0)
+    for (int k = 0; k < D; k++) { smin[w][k] = lo[k]; smax[w][k] = hi[k]; ssum[w][k] = s[k]; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     for (int k = 0; k < D; k++) {
+      lo[k] = INFINITY; hi[k] = -INFINITY; s[k] = 0;
+      for (int j = 0; j < SGT_THREADS / 32; j++) {
+        lo[k] = fminf(lo[k], smin[j][k]);
+        hi[k] = fmaxf(hi[k], smax[j][k]);
+        s[k] += ssum[j][k];
+      }
       st->minv[k] = lo[k];
       st->maxv[k] = hi[k];
       st->sum[k] = s[k];
@@ -184,6 +155,203 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
     st->iter = iter + 1;
     st->done_row = 0;
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused iteration row kernel.  FUSED: compute F_attr from CSR; otherwise read
+// it from Fattr (COO / ELL formats).  Writes Ynext, uY, gains; the last CTA
+// turns the per-block min/max/sum of Ynext into the next grid decision.
+// ---------------------------------------------------------------------------
+template <int D, int G, bool FUSED>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+             const typename Vec<D>::T *__restrict__ Fattr,
+             const typename Vec<D>::T *__restrict__ Y,
+             const typename Vec<D>::T *__restrict__ Frep_un,
+             typename Vec<D>::T *__restrict__ uY,
+             typename Vec<D>::T *__restrict__ gains,
+             typename Vec<D>::T *__restrict__ Ynext, SgtState *st,
+             SgtJobParams jp, float4 *part_min, float4 *part_max,
+             double *part_sum) {
+  const int n = jp.n;
+  const int iter = st->iter;
+  const float alpha = iter <= jp.early_iter ? jp.alpha0 : 1.0f;
+  const float mom = iter <= jp.mom_switch ? 0.5f : 0.8f;
+  const float eta = jp.eta;
+  const float Zf = (float)st->Z;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double sm[3] = {0, 0, 0};
+  const int lane = threadIdx.x % G;
+  const int grp = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int ngrp = gridDim.x * blockDim.x / G;
+  // uniform trip count per warp so the group shuffles stay converged
+  const int rounds = (n + ngrp - 1) / ngrp;
+  // the next row's extents are loaded one round ahead
+  int nb_s = 0, nb_e = 0;
+  if (FUSED && grp < n) {
+    nb_s = __ldcs(&rowptr[grp]);
+    nb_e = __ldcs(&rowptr[grp + 1]);
+  }
+  for (int r = 0; r < rounds; r++) {
+    const int i = grp + r * ngrp;
+    const bool valid = i < n;
+    const int rs = nb_s, re = nb_e;
+    if (FUSED && i + ngrp < n) {
+      nb_s = __ldcs(&rowptr[i + ngrp]);
+      nb_e = __ldcs(&rowptr[i + ngrp + 1]);
+    }
+    typename Vec<D>::T yi, fr, u, g;
+    if (valid) {
+      yi = Y[i];
+      if (lane == 0) {  // update operands, independent of the row sum
+        fr = __ldcs(&Frep_un[i]);
+        u = __ldcs(&uY[i]);
+        g = __ldcs(&gains[i]);
+      }
+    }
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (FUSED) {
+      if (valid) {
+        constexpr int U = 4;
+        for (int t0 = rs + lane; t0 < re; t0 += U * G) {
+          int2 pr[U];
+#pragma unroll
+          for (int q = 0; q < U; q++) {
+            const int t = t0 + q * G;
+            pr[q] = t < re ? __ldcs(&pairs[t]) : make_int2(i, 0);
+          }
+          typename Vec<D>::T yj[U];
+#pragma unroll
+          for (int q = 0; q < U; q++) yj[q] = __ldg(&Y[pr[q].x]);
+#pragma unroll
+          for (int q = 0; q < U; q++) attr_term<D>(yi, yj[q], __int_as_float(pr[q].y), acc);
+        }
+      }
+      group_reduce<D, G>(acc);
+    } else if (valid) {
+      const typename Vec<D>::T fa = Fattr[i];
+#pragma unroll
+      for (int k = 0; k < D; k++) acc[k] = comp<D>(fa, k);
+    }
+    if (valid && lane == 0) {
+      typename Vec<D>::T yn = yi;
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        const float frep = comp<D>(fr, k) / Zf;
+        const float dy = alpha * acc[k] - frep;
+        float gk = comp<D>(g, k), uk = comp<D>(u, k);
+        gk = (sgn_f(dy) != sgn_f(uk)) ? (float)((double)gk + 0.2) : (float)((double)gk * 0.8);
+        if ((double)gk < 0.01) gk = (float)0.01;
+        uk = mom * uk - eta * gk * dy;
+        const float y = comp<D>(yi, k) + uk;
+        setcomp<D>(g, k, gk);
+        setcomp<D>(u, k, uk);
+        setcomp<D>(yn, k, y);
+        mn[k] = fminf(mn[k], y);
+        mx[k] = fmaxf(mx[k], y);
+        sm[k] += (double)y;
+      }
+      if constexpr (D == 3) { u.w = 0.f; g.w = 0.f; yn.w = 0.f; }
+      __stcs(&uY[i], u);
+      __stcs(&gains[i], g);
+      Ynext[i] = yn;
+    }
+  }
+  block_finish_stats<D>(st, jp, mn, mx, sm, part_min, part_max, part_sum, iter, alpha, mom);
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused CSR row kernel, one row per G-lane group, launched over all rows
+// (ceil(n G / 256) blocks): the hardware refills SMs as blocks retire, so a
+// long row delays one group, not a persistent warp.  Kept lean (no loop
+// state across rows) so 48+ warps stay resident per SM.
+// ---------------------------------------------------------------------------
+template <int D, int G>
+__global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
+k_row_fused(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+            const typename Vec<D>::T *__restrict__ Y,
+            const typename Vec<D>::T *__restrict__ Frep_un,
+            typename Vec<D>::T *__restrict__ uY, typename Vec<D>::T *__restrict__ gains,
+            typename Vec<D>::T *__restrict__ Ynext, SgtState *st, SgtJobParams jp,
+            float4 *part_min, float4 *part_max, double *part_sum) {
+  const int n = jp.n;
+  const int lane = threadIdx.x % G;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool valid = i < n;
+  float acc[3] = {0.f, 0.f, 0.f};
+  typename Vec<D>::T yi;
+  if (valid) {
+    const int rs = __ldcs(&rowptr[i]), re = __ldcs(&rowptr[i + 1]);
+    yi = Y[i];
+    constexpr int U = 4;
+    for (int t0 = rs + lane; t0 < re; t0 += U * G) {
+      int2 pr[U];
+#pragma unroll
+      for (int q = 0; q < U; q++) {
+        const int t = t0 + q * G;
+        pr[q] = t < re ? __ldcs(&pairs[t]) : make_int2(i, 0);
+      }
+      typename Vec<D>::T yj[U];
+#pragma unroll
+      for (int q = 0; q < U; q++) yj[q] = __ldg(&Y[pr[q].x]);
+#pragma unroll
+      for (int q = 0; q < U; q++) attr_term<D>(yi, yj[q], __int_as_float(pr[q].y), acc);
+    }
+  }
+  group_reduce<D, G>(acc);
+  if (valid && lane == 0) {
+    const int iter = st->iter;
+    const float alpha = iter <= jp.early_iter ? jp.alpha0 : 1.0f;
+    const float mom = iter <= jp.mom_switch ? 0.5f : 0.8f;
+    const float Zf = (float)st->Z;
+    const typename Vec<D>::T fr = __ldcs(&Frep_un[i]);
+    typename Vec<D>::T u = __ldcs(&uY[i]), g = __ldcs(&gains[i]), yn = yi;
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      const float frep = comp<D>(fr, k) / Zf;
+      const float dy = alpha * acc[k] - frep;
+      float gk = comp<D>(g, k), uk = comp<D>(u, k);
+      gk = (sgn_f(dy) != sgn_f(uk)) ? (float)((double)gk + 0.2) : (float)((double)gk * 0.8);
+      if ((double)gk < 0.01) gk = (float)0.01;
+      uk = mom * uk - jp.eta * gk * dy;
+      setcomp<D>(g, k, gk);
+      setcomp<D>(u, k, uk);
+      setcomp<D>(yn, k, comp<D>(yi, k) + uk);
+    }
+    if constexpr (D == 3) { u.w = 0.f; g.w = 0.f; yn.w = 0.f; }
+    __stcs(&uY[i], u);
+    __stcs(&gains[i], g);
+    Ynext[i] = yn;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// End of an iteration: min/max/sum of Ynext, the next grid decision and the
+// schedule (alpha after early_iter, momentum after iteration 250).  The row
+// kernel stays free of block-wide synchronisation.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_iter_stats(const typename Vec<D>::T *__restrict__ Ynext, SgtState *st, SgtJobParams jp,
+             float4 *part_min, float4 *part_max, double *part_sum) {
+  const int iter = st->iter;
+  const float alpha = iter <= jp.early_iter ? jp.alpha0 : 1.0f;
+  const float mom = iter <= jp.mom_switch ? 0.5f : 0.8f;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double sm[3] = {0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < jp.n; i += gridDim.x * blockDim.x) {
+    const typename Vec<D>::T y = Ynext[i];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      const float v = comp<D>(y, k);
+      mn[k] = fminf(mn[k], v);
+      mx[k] = fmaxf(mx[k], v);
+      sm[k] += (double)v;
+    }
+  }
+  block_finish_stats<D>(st, jp, mn, mx, sm, part_min, part_max, part_sum, iter, alpha, mom);
 }
 
 // ---------------------------------------------------------------------------
@@ -359,3 +527,13 @@ __global__ void k_unpack(const typename Vec<D>::T *__restrict__ src, int n,
     }
   }
 }
+
+// dst[r] = src[perm[r]] (user order -> engine order), Vec<D> arrays
+template <int D>
+__global__ void k_permute_vec(const typename Vec<D>::T *__restrict__ src,
+                              const int *__restrict__ perm, int n,
+                              typename Vec<D>::T *__restrict__ dst) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    dst[r] = src[perm[r]];
+}
+

@@ -137,6 +137,8 @@ typedef struct {
   double kl;         /* last KL value recorded (kl_every > 0)     */
   int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
   long nnz;          /* nonzeros of P                             */
+  int row_group;     /* lanes per row picked by the autotuner      */
+  float tune_ms[4];  /* row kernel ms measured for 4, 8, 16, 32 lanes */
 } sgt_job_info;
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */

@@ -280,13 +280,50 @@ static inline void weights(double s, uint32_t *f, double w[4]) {
 
 /* S2G: V[c][z][y][x] += q_c * wx*wy*wz (HYB/gridding.cpp:57-101,164-221,298-368
    with np = 1, i.e. one private grid). */
+static void s2g_range(int i0, int i1, int d, int N, const double *ys,
+                      const double *q, double *V);
+
 void orc_s2g(int n, int d, int N, const double *ys, const double *q,
              double *V) {
+  /* np private grids reduced at the end, as HYB/nuconv.cpp:52-86 */
   int m = d + 1;
   long G = 1;
   for (int k = 0; k < d; k++) G *= N;
   memset(V, 0, sizeof(double) * (size_t)(G * m));
-  for (int i = 0; i < n; i++) {
+  int np = 1;
+#ifdef _OPENMP
+  np = omp_get_max_threads();
+  if ((long)n < 20000L * np) np = 1;
+#endif
+  if (np == 1) {
+    s2g_range(0, n, d, N, ys, q, V);
+    return;
+  }
+  double *priv = (double *)calloc((size_t)np * G * m, sizeof(double));
+#pragma omp parallel num_threads(np)
+  {
+    int t = 0;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+#endif
+    int i0 = (int)((long)n * t / np), i1 = (int)((long)n * (t + 1) / np);
+    s2g_range(i0, i1, d, N, ys, q, priv + (size_t)t * G * m);
+  }
+#pragma omp parallel for schedule(static)
+  for (long g = 0; g < G * m; g++) {
+    double acc = 0;
+    for (int t = 0; t < np; t++) acc += priv[(size_t)t * G * m + g];
+    V[g] = acc;
+  }
+  free(priv);
+}
+
+static void s2g_range(int i0, int i1, int d, int N, const double *ys,
+                      const double *q, double *V) {
+  int m = d + 1;
+  long G = 1;
+  for (int k = 0; k < d; k++) G *= N;
+  for (int i = i0; i < i1; i++) {
     uint32_t f[3] = {0, 0, 0};
     double w[3][4] = {{1, 0, 0, 0}, {1, 0, 0, 0}, {1, 0, 0, 0}};
     for (int k = 0; k < d; k++) weights(ys[(long)i * d + k], &f[k], w[k]);
@@ -805,6 +842,7 @@ void orc_lambda_rescale(int n, const int *rowptr, double *val, double lambda,
                         int dist, double *sigma_out) {
   const double tol = 1e-5;
   const int max_iter = 100;
+#pragma omp parallel for schedule(dynamic, 1024)
   for (int i = 0; i < n; i++) {
     double fval = 1 - lambda, sig = 1, a = -1e3, c = INFINITY, sum = 0;
     int iter = 0;

