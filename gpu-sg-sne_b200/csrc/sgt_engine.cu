@@ -13,6 +13,7 @@
 #include "sgt_grid.cuh"
 #include "sgt_prep.cuh"
 #include "sgt_rows.cuh"
+#include "sgt_relayout.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -49,6 +50,14 @@ struct sgt_job {
   float *ell_vals = nullptr;
   int ell_w = 0;
   int *perm = nullptr;  // engine slot -> caller's point index (nullptr: identity)
+  // locality relabelling (CSR format): scratch allocated on first use
+  int *rowptr_alt = nullptr, *perm_alt = nullptr, *rl_p = nullptr, *rl_iperm = nullptr,
+      *rl_hist = nullptr, *rl_len = nullptr, *rl_bsum = nullptr;
+  unsigned *rl_keys = nullptr;
+  int2 *pairs_alt = nullptr;
+  float *gains_alt = nullptr;
+  long host_iter = 0;  // iterations since the last set_y
+  int relayouts = 0;
   float *Y = nullptr, *Ynext = nullptr, *uY = nullptr, *gains = nullptr,
         *Frep = nullptr, *Fattr = nullptr;
   float4 *sorted = nullptr;
@@ -61,7 +70,7 @@ struct sgt_job {
   double *part_sum = nullptr, *part_z = nullptr, *part_kl = nullptr;
   SgtState *st = nullptr;
   SgtState *st_host = nullptr;
-  int nb_pts = 0, nb_s2g = 0, nb_g2s = 0, nb_fft = 0, nb_row = 0, nb_part = 0;
+  int nb_pts = 0, nb_s2g = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0, nb_part = 0;
   size_t smem_s2g = 0, smem_fft1 = 0, smem_fft2 = 0;
   cudaGraphExec_t gexec = nullptr;
   std::vector<void *> allocs;
@@ -120,6 +129,7 @@ void sgt_params_default(sgt_params *p) {
   p->grid_mode = SGT_GRID_H;
   p->lambda_dist = 1;
   p->seed = 0;
+  p->relayout_every = 0;
 }
 
 int sgt_abi_version(void) { return SGT_ABI_VERSION; }
@@ -250,20 +260,20 @@ static sgt_status job_shapes(sgt_job *J) {
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2s<D>, SGT_THREADS, 0));
   J->nb_g2s = grid_blocks(nsm, occ);
   const int M = J->mmax;
-  J->smem_fft1 = sizeof(float2) * (512 + (size_t)SGT_FFT_LINES * (M + 1));
-  J->smem_fft2 = sizeof(float2) * (512 + 2 * (size_t)SGT_FFT_LINES * (M + 1));
+  J->smem_fft1 = 0;
+  J->smem_fft2 = fft_cols_smem(M);
   if constexpr (D == 1) {
-    J->smem_fft2 = sizeof(float2) * (512 + 2 * (size_t)(M + 1));
-    CK(cudaFuncSetAttribute(k_conv1d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
     J->nb_fft = 1;
   } else {
-    CK(cudaFuncSetAttribute(k_fft_build_x<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft1));
-    CK(cudaFuncSetAttribute(k_fft_last<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
-    CK(cudaFuncSetAttribute(k_fft_final_x<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
-    if constexpr (D == 3)
-      CK(cudaFuncSetAttribute(k_fft_mid_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft1));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fft_last<D>, SGT_THREADS, J->smem_fft2));
+    CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+    if constexpr (D == 3) {
+      CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_MID_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+      CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_MID_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+    }
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fft_cols<D, MODE_LAST>, SGT_THREADS, J->smem_fft2));
     J->nb_fft = grid_blocks(nsm, occ);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fft_build_x<D>, SGT_THREADS, 0));
+    J->nb_fft_rows = grid_blocks(nsm, occ);
   }
   occ = 0;
   switch (J->G) {
@@ -376,6 +386,23 @@ static sgt_status job_new(sgt_ctx *ctx, const sgt_params *p, int n, sgt_job **ou
 // iteration enqueue
 // ---------------------------------------------------------------------------
 template <int D>
+static sgt_status enqueue_g2g(sgt_job *J, cudaStream_t s) {
+  typedef typename Node<D>::T NT;
+  if constexpr (D == 1) {
+    k_conv1d<<<1, 32, 0, s>>>(J->st, (const float2 *)J->V, (float2 *)J->Phi);
+  } else {
+    k_fft_build_x<D><<<J->nb_fft_rows, SGT_THREADS, 0, s>>>(J->st, (const NT *)J->V, J->W);
+    if constexpr (D == 3)
+      k_fft_cols<D, MODE_MID_FWD><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+    k_fft_cols<D, MODE_LAST><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+    if constexpr (D == 3)
+      k_fft_cols<D, MODE_MID_INV><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+    k_fft_final_x<D><<<J->nb_fft_rows, SGT_THREADS, 0, s>>>(J->st, J->W, (NT *)J->Phi);
+  }
+  return SGT_OK;
+}
+
+template <int D>
 static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
@@ -387,15 +414,7 @@ static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s) {
   k_bin_scatter<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, n, J->st, J->cursor,
                                                      J->sorted);
   k_s2g<D><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
-  if constexpr (D == 1) {
-    k_conv1d<<<1, SGT_THREADS, J->smem_fft2, s>>>(J->st, (const float2 *)J->V, (float2 *)J->Phi);
-  } else {
-    k_fft_build_x<D><<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, (const NT *)J->V, J->W);
-    if constexpr (D == 3) k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 0);
-    k_fft_last<D><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
-    if constexpr (D == 3) k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 1);
-    k_fft_final_x<D><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W, (NT *)J->Phi);
-  }
+  CKS(enqueue_g2g<D>(J, s));
   k_g2s<D><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi,
                                              (VT *)J->Frep, J->part_z, n);
   CK(cudaGetLastError());
@@ -626,6 +645,88 @@ static sgt_status tune_group(sgt_job *J) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// locality relabelling (see sgt_relayout.cuh); runs between iterations
+// ---------------------------------------------------------------------------
+static sgt_status scan_exclusive(sgt_job *J, const int *in, int len, int *out, int *total,
+                                 cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  const int nb = (len + SGT_SCAN_PER_BLOCK - 1) / SGT_SCAN_PER_BLOCK;
+  if (nb > 4096) return fail(ctx, SGT_ERR_UNSUPPORTED, "scan longer than 16M items");
+  k_scan_blocks<<<nb, 1024, 0, s>>>(in, len, out, J->rl_bsum);
+  k_scan_sums<<<1, 1024, 0, s>>>(J->rl_bsum, nb, total);
+  k_scan_add<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(out, len, J->rl_bsum);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+template <int D>
+static sgt_status relayout_d(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  typedef typename Vec<D>::T VT;
+  const int n = J->n;
+  const int KEYS = 1 << 18;
+  if (!J->rl_p) {
+    CKS(jalloc(J, &J->rowptr_alt, (size_t)n + 1));
+    CKS(jalloc(J, &J->pairs_alt, (size_t)J->nnz + 8));
+    CKS(jalloc(J, &J->perm_alt, (size_t)n));
+    CKS(jalloc(J, &J->rl_p, (size_t)n));
+    CKS(jalloc(J, &J->rl_iperm, (size_t)n));
+    CKS(jalloc(J, &J->rl_len, (size_t)n + 1));
+    CKS(jalloc(J, &J->rl_hist, (size_t)KEYS + 1));
+    CKS(jalloc(J, &J->rl_bsum, 4096));
+    CKS(jalloc(J, &J->rl_keys, (size_t)n));
+    CKS(jalloc(J, &J->gains_alt, (size_t)n * J->S));
+    CK(cudaMemsetAsync(J->pairs_alt + J->nnz, 0, 8 * sizeof(int2), s));
+  }
+  const int nb = grid_blocks(ctx->nsm, 4);
+  CK(cudaMemsetAsync(J->rl_hist, 0, sizeof(int) * KEYS, s));
+  k_cell_keys<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, n, J->st, J->rl_keys, J->rl_hist);
+  CKS(scan_exclusive(J, J->rl_hist, KEYS, J->rl_hist, nullptr, s));
+  k_key_scatter<<<nb, SGT_THREADS, 0, s>>>(J->rl_keys, n, J->rl_hist, J->rl_p);
+  k_perm_prep<<<nb, SGT_THREADS, 0, s>>>(J->rl_p, n, J->rowptr, J->rl_iperm, J->rl_len, J->perm,
+                                         J->perm_alt);
+  CKS(scan_exclusive(J, J->rl_len, n, J->rowptr_alt, J->rowptr_alt + n, s));
+  k_relabel_rows<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, s>>>(
+      J->rl_p, J->rl_iperm, n, J->rowptr, J->pairs, J->rowptr_alt, J->pairs_alt);
+  // per-point state (all n*S floats): Ynext into the free Y buffer (the next
+  // binning rewrites Y), uY into the free F_rep buffer (the next G2S rewrites
+  // it), gains into its own spare buffer; then swap the roles
+  k_gather_vec<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, J->rl_p, n, (VT *)J->Y);
+  k_gather_vec<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->uY, J->rl_p, n, (VT *)J->Frep);
+  k_gather_vec<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->gains, J->rl_p, n, (VT *)J->gains_alt);
+  CK(cudaGetLastError());
+  std::swap(J->Y, J->Ynext);
+  std::swap(J->uY, J->Frep);
+  std::swap(J->gains, J->gains_alt);
+  std::swap(J->rowptr, J->rowptr_alt);
+  std::swap(J->pairs, J->pairs_alt);
+  if (J->perm) {
+    std::swap(J->perm, J->perm_alt);
+  } else {
+    J->perm = J->perm_alt;
+    J->perm_alt = nullptr;
+    CKS(jalloc(J, &J->perm_alt, (size_t)n));
+  }
+  if (J->gexec) {  // buffers moved: capture the iteration again
+    cudaGraphExecDestroy(J->gexec);
+    J->gexec = nullptr;
+  }
+  J->relayouts++;
+  return SGT_OK;
+}
+
+static sgt_status relayout(sgt_job *J) {
+  if (J->format != SGT_FORMAT_CSR || J->n > (16 << 20)) return SGT_OK;
+  switch (J->d) {
+    case 1: return relayout_d<1>(J);
+    case 2: return relayout_d<2>(J);
+    default: return relayout_d<3>(J);
+  }
+}
+
 extern "C" {
 
 // ---------------------------------------------------------------------------
@@ -828,7 +929,8 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
   }
   CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
   CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, s));
-  CKS(init_stats(J, s, J->p.grid_mode == SGT_GRID_H ? 1 : 1));
+  CKS(init_stats(J, s, 1));
+  J->host_iter = 0;
   if (staging) {
     CK(cudaStreamSynchronize(s));
     CK(cudaFree(staging));
@@ -836,10 +938,28 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
   return SGT_OK;
 }
 
+static sgt_status run_one(sgt_job *J);
 sgt_status sgt_job_run(sgt_job *J, int iters) {
   if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
   sgt_ctx *ctx = J->ctx;
   CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const int every = J->p.relayout_every;
+  for (int it = 0; it < iters; it++) {
+    if (every > 0 && J->host_iter > 0 && J->host_iter % every == 0) CKS(relayout(J));
+    CKS(run_one(J));
+    J->host_iter++;
+    if (J->p.kl_every > 0 && (J->host_iter % J->p.kl_every) == 0) {
+      double kl = 0;
+      // KL of the coordinates the step just used (Y) with that step's Z
+      CKS(sgt_job_kl(J, -1.0, &kl));
+    }
+  }
+  return SGT_OK;
+}
+
+static sgt_status run_one(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
   cudaStream_t s = ctx->stream;
   if (!J->gexec) {
     cudaGraph_t g = nullptr;
@@ -855,16 +975,7 @@ sgt_status sgt_job_run(sgt_job *J, int iters) {
     cudaGraphDestroy(g);
     CK(ie);
   }
-  const int kl_every = J->p.kl_every;
-  for (int it = 0; it < iters; it++) {
-    CK(cudaGraphLaunch(J->gexec, s));
-    if (kl_every > 0 && ((it + 1) % kl_every) == 0) {
-      double kl = 0;
-      // KL of the coordinates the step just used (Y) with that step's Z
-      sgt_status ks = sgt_job_kl(J, -1.0, &kl);
-      if (ks != SGT_OK) return ks;
-    }
-  }
+  CK(cudaGraphLaunch(J->gexec, s));
   return SGT_OK;
 }
 
@@ -967,7 +1078,7 @@ sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
         CK(cudaEventRecord(ev[1], s));
         k_s2g<1><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
         CK(cudaEventRecord(ev[2], s));
-        k_conv1d<<<1, SGT_THREADS, J->smem_fft2, s>>>(J->st, (const float2 *)J->V, (float2 *)J->Phi);
+        CKS(enqueue_g2g<1>(J, s));
         CK(cudaEventRecord(ev[3], s));
         k_g2s<1><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
         break;
@@ -980,9 +1091,7 @@ sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
         CK(cudaEventRecord(ev[1], s));
         k_s2g<2><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
         CK(cudaEventRecord(ev[2], s));
-        k_fft_build_x<2><<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, (const NT *)J->V, J->W);
-        k_fft_last<2><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
-        k_fft_final_x<2><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W, (NT *)J->Phi);
+        CKS(enqueue_g2g<2>(J, s));
         CK(cudaEventRecord(ev[3], s));
         k_g2s<2><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
         break;
@@ -995,11 +1104,7 @@ sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
         CK(cudaEventRecord(ev[1], s));
         k_s2g<3><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
         CK(cudaEventRecord(ev[2], s));
-        k_fft_build_x<3><<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, (const NT *)J->V, J->W);
-        k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 0);
-        k_fft_last<3><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
-        k_fft_mid_y<<<J->nb_fft, SGT_THREADS, J->smem_fft1, s>>>(J->st, J->W, 1);
-        k_fft_final_x<3><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W, (NT *)J->Phi);
+        CKS(enqueue_g2g<3>(J, s));
         CK(cudaEventRecord(ev[3], s));
         k_g2s<3><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
         break;

@@ -5,29 +5,38 @@
 // with cuFFT (CU/non_periodic_convF.cu:14-517, HYB/non_periodic_conv.cpp);
 // the sum of those terms is exactly the aperiodic convolution.  Here the
 // same convolution is one cyclic convolution of length M = 2^k >= 2N-1 per
-// axis: for output nodes x < N only kernel offsets |x - x'| <= N-1 <= M/2
-// are touched, so K_c[r] = K(min(r, M-r)) reproduces it.  Two real charge
-// channels ride in one complex plane (K_c is real and even, so its FFT is
-// real and the channels separate after the inverse transform).
+// axis: output nodes x < N only meet kernel offsets |x - x'| <= N-1 <= M/2,
+// so K_c[r] = K(min(r, M-r)) reproduces it.  Two real charge channels ride in
+// one complex plane (K_c is real and even, so its transform is real and the
+// channels separate after the inverse).
 //
-// Each pass transforms blocks of SGT_FFT_LINES lines in shared memory with a
-// radix-2 FFT written here (decimation in time for forward transforms with a
-// bit-reversed load, decimation in frequency for inverse transforms with a
-// bit-reversed read-out).  Lines along y/z are taken 8 adjacent x positions
-// at a time so every global access is a 64-byte segment.  Planes of zero
-// charge (index >= N) are never stored or read.  Passes are persistent
-// (fixed grid, loop over work items sized from the device-side grid
-// decision), so the chain replays inside a CUDA graph as N changes.
+// FFTs are register-resident: one warp owns one line of M <= 1024 points, a
+// lane holds the E = M/32 points lane + 32 e; butterflies with span >= 32
+// stay inside a lane, shorter spans use warp shuffles.  Forward transforms
+// are decimation in frequency (natural order in, bit-reversed out) and
+// inverse transforms decimation in time (bit-reversed in, natural out), so
+// spectra stay bit-reversed in memory and no permutation pass exists.  Rows
+// are read and written directly (coalesced); columns go through a shared
+// memory transpose of 8 adjacent columns so every global access is a 64-byte
+// segment.  Planes of zero charge (index >= N) are never stored or read.
+// Kernels are persistent and size their work from the device-side grid
+// decision, so the chain replays inside a CUDA graph as N changes.
 #pragma once
 #include "sgt_common.cuh"
 
-#define SGT_LS(M) ((M) + 1)  // padded line stride in float2
+#define SGT_FFT_COLS 8  // columns per CTA in column passes (one per warp)
+#define SGT_FFT_PAD 1   // float2 padding per staged column
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 shfl_x2(float2 v, int m) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
 
-// tw[j] = exp(-2 pi i j / M), j < M/2
+// tw[j] = exp(-2 pi i j / M), j < M/2 (accurate sincospi)
 __device__ __forceinline__ void fft_twiddles(float2 *tw, int M) {
   for (int j = threadIdx.x; j < (M >> 1); j += blockDim.x) {
     float s, c;
@@ -36,49 +45,67 @@ __device__ __forceinline__ void fft_twiddles(float2 *tw, int M) {
   }
 }
 
-__device__ __forceinline__ int brev(int x, int logM) {
-  return (int)(__brev((unsigned)x) >> (32 - logM));
-}
-
-// forward DIT, bit-reversed input -> natural output
-__device__ void fft_dit(float2 *buf, int lines, int M, int logM,
-                        const float2 *tw) {
-  const int half = M >> 1, ls = SGT_LS(M);
-  for (int s = 0; s < logM; s++) {
-    const int hs = 1 << s, tsh = logM - 1 - s;
-    for (int b = threadIdx.x; b < lines * half; b += blockDim.x) {
-      const int l = b >> (logM - 1), k = b & (half - 1);
-      const int pos = k & (hs - 1);
-      const int i0 = ((k >> s) << (s + 1)) + pos, i1 = i0 + hs;
-      float2 *L = buf + l * ls;
-      const float2 w = tw[pos << tsh];
-      const float2 u = L[i0], v = cmul(L[i1], w);
-      L[i0] = make_float2(u.x + v.x, u.y + v.y);
-      L[i1] = make_float2(u.x - v.x, u.y - v.y);
+// forward DIF: natural order in, bit-reversed out (position i holds X[brev i])
+template <int LOGM>
+__device__ __forceinline__ void wfft_dif(float2 *v, const float2 *__restrict__ tw) {
+  constexpr int E = (1 << LOGM) / 32;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = LOGM - 1; s >= 0; s--) {
+    const int hs = 1 << s, sh = LOGM - 1 - s;
+    if (hs >= 32) {
+      const int he = hs >> 5;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        if ((e & he) == 0) {
+          const float2 w = tw[((lane + 32 * e) & (hs - 1)) << sh];
+          const float2 u = v[e], t = v[e + he];
+          v[e] = cadd(u, t);
+          v[e + he] = cmul(csub(u, t), w);
+        }
+      }
+    } else {
+      const bool upper = (lane & hs) != 0;
+      const float2 w = tw[(lane & (hs - 1)) << sh];
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const float2 x = v[e], y = shfl_x2(x, hs);
+        v[e] = upper ? cmul(csub(y, x), w) : cadd(x, y);
+      }
     }
-    __syncthreads();
   }
 }
 
-// inverse DIF (conjugate twiddles, no scaling), natural input ->
-// bit-reversed output
-__device__ void fft_dif_inv(float2 *buf, int lines, int M, int logM,
-                            const float2 *tw) {
-  const int half = M >> 1, ls = SGT_LS(M);
-  for (int s = logM - 1; s >= 0; s--) {
-    const int hs = 1 << s, tsh = logM - 1 - s;
-    for (int b = threadIdx.x; b < lines * half; b += blockDim.x) {
-      const int l = b >> (logM - 1), k = b & (half - 1);
-      const int pos = k & (hs - 1);
-      const int i0 = ((k >> s) << (s + 1)) + pos, i1 = i0 + hs;
-      float2 *L = buf + l * ls;
-      float2 w = tw[pos << tsh];
+// inverse DIT (conjugate twiddles, unscaled): bit-reversed in, natural out
+template <int LOGM>
+__device__ __forceinline__ void wfft_dit_inv(float2 *v, const float2 *__restrict__ tw) {
+  constexpr int E = (1 << LOGM) / 32;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 0; s < LOGM; s++) {
+    const int hs = 1 << s, sh = LOGM - 1 - s;
+    if (hs >= 32) {
+      const int he = hs >> 5;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        if ((e & he) == 0) {
+          float2 w = tw[((lane + 32 * e) & (hs - 1)) << sh];
+          w.y = -w.y;
+          const float2 u = v[e], t = cmul(v[e + he], w);
+          v[e] = cadd(u, t);
+          v[e + he] = csub(u, t);
+        }
+      }
+    } else {
+      const bool upper = (lane & hs) != 0;
+      float2 w = tw[(lane & (hs - 1)) << sh];
       w.y = -w.y;
-      const float2 u = L[i0], v = L[i1];
-      L[i0] = make_float2(u.x + v.x, u.y + v.y);
-      L[i1] = cmul(make_float2(u.x - v.x, u.y - v.y), w);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const float2 x = v[e], y = shfl_x2(x, hs);
+        v[e] = upper ? csub(y, cmul(x, w)) : cadd(x, cmul(y, w));
+      }
     }
-    __syncthreads();
   }
 }
 
@@ -89,261 +116,289 @@ __device__ __forceinline__ float kern_val(float hsq, int M, int x, int y, int z)
   return 1.0f / (b * b);
 }
 
-// number of data planes (complex) for d: pairs of the d+1 real channels
-template <int D> struct Planes { static constexpr int n = D == 1 ? 1 : 2; };
-
 template <int D>
 __device__ __forceinline__ float2 node_plane(const typename Node<D>::T &v, int p) {
   if constexpr (D == 1) return v;
   else return p == 0 ? make_float2(v.x, v.y) : make_float2(v.z, D == 3 ? v.w : 0.f);
 }
 
+#define SGT_FFT_DISPATCH(LOGM_EXPR, CALL)         \
+  switch (LOGM_EXPR) {                            \
+    case 5: CALL(5); break;                       \
+    case 6: CALL(6); break;                       \
+    case 7: CALL(7); break;                       \
+    case 8: CALL(8); break;                       \
+    case 9: CALL(9); break;                       \
+    default: CALL(10); break;                     \
+  }
+
 // ---------------------------------------------------------------------------
-// d = 1: whole convolution in one CTA
+// d = 1: the whole convolution in one warp
 // ---------------------------------------------------------------------------
+template <int LOGM>
+__device__ void conv1d_body(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi,
+                            const float2 *tw) {
+  constexpr int M = 1 << LOGM, E = M / 32;
+  const int N = st->N, lane = threadIdx.x & 31;
+  const float hsq = st->h_eff * st->h_eff;
+  float2 k[E], v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int x = lane + 32 * e;
+    k[e] = make_float2(kern_val(hsq, M, x, 0, 0), 0.f);
+    v[e] = x < N ? V[x] : make_float2(0.f, 0.f);
+  }
+  wfft_dif<LOGM>(k, tw);
+  wfft_dif<LOGM>(v, tw);
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = make_float2(v[e].x * k[e].x, v[e].y * k[e].x);
+  wfft_dit_inv<LOGM>(v, tw);
+  const float inv = 1.0f / (float)M;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int x = lane + 32 * e;
+    if (x < N) Phi[x] = make_float2(v[e].x * inv, v[e].y * inv);
+  }
+}
+
 __global__ void __launch_bounds__(SGT_THREADS)
 k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi) {
-  extern __shared__ float2 sm[];
-  const int N = st->N, M = st->M, logM = st->logM;
-  const float hsq = st->h_eff * st->h_eff;
-  float2 *tw = sm, *bk = sm + 512, *bd = bk + SGT_LS(M);
-  fft_twiddles(tw, M);
-  for (int x = threadIdx.x; x < M; x += blockDim.x) {
-    const int r = brev(x, logM);
-    bk[r] = make_float2(kern_val(hsq, M, x, 0, 0), 0.f);
-    bd[r] = x < N ? V[x] : make_float2(0.f, 0.f);
-  }
+  __shared__ float2 tw[512];
+  fft_twiddles(tw, st->M);
   __syncthreads();
-  fft_dit(bk, 1, M, logM, tw);
-  fft_dit(bd, 1, M, logM, tw);
-  for (int x = threadIdx.x; x < M; x += blockDim.x) {
-    const float kr = bk[x].x;
-    bd[x] = make_float2(bd[x].x * kr, bd[x].y * kr);
-  }
-  __syncthreads();
-  fft_dif_inv(bd, 1, M, logM, tw);
-  const float inv = 1.0f / (float)M;
-  for (int x = threadIdx.x; x < N; x += blockDim.x) {
-    const float2 v = bd[brev(x, logM)];
-    Phi[x] = make_float2(v.x * inv, v.y * inv);
-  }
+  if (threadIdx.x >= 32) return;
+#define C1(L) conv1d_body<L>(st, V, Phi, tw)
+  SGT_FFT_DISPATCH(st->logM, C1)
+#undef C1
 }
 
 // ---------------------------------------------------------------------------
-// d >= 2, pass 1: build rows (x lines) of the data planes and of the kernel
-// plane, forward FFT along x.
-// W plane p at W + p*M^d; kernel plane index Planes<D>::n.
+// d >= 2, pass 1: build rows (x lines) of the data planes (rows y, z < N) and
+// of the kernel plane (all rows), forward FFT along x.
+// W plane p at W + p * M^d; the kernel plane is p = 2.
 // ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V,
-              float2 *__restrict__ W) {
-  extern __shared__ float2 sm[];
-  const int N = st->N, M = st->M, logM = st->logM;
+template <int D, int LOGM>
+__device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *__restrict__ V,
+                                float2 *__restrict__ W, const float2 *tw) {
+  constexpr int M = 1 << LOGM, E = M / 32;
+  const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float hsq = st->h_eff * st->h_eff;
-  constexpr int P = Planes<D>::n;
   const long plane = D == 2 ? (long)M * M : (long)M * M * M;
-  float2 *tw = sm, *buf = sm + 512;
-  fft_twiddles(tw, M);
-  const int nyb_d = (N + SGT_FFT_LINES - 1) / SGT_FFT_LINES;
-  const int nz_d = D == 3 ? N : 1;
-  const int nyb_k = M / SGT_FFT_LINES;
-  const int nz_k = D == 3 ? M : 1;
-  const int items_d = P * nyb_d * nz_d, items = items_d + nyb_k * nz_k;
-  const int ls = SGT_LS(M);
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    int p, z, y0;
-    const bool isk = it >= items_d;
-    if (!isk) {
-      p = it / (nyb_d * nz_d);
-      const int r = it % (nyb_d * nz_d);
-      z = r / nyb_d;
-      y0 = (r % nyb_d) * SGT_FFT_LINES;
-    } else {
-      p = P;
-      const int r = it - items_d;
-      z = r / nyb_k;
-      y0 = (r % nyb_k) * SGT_FFT_LINES;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < SGT_FFT_LINES * M; e += blockDim.x) {
-      const int l = e / M, x = e % M, y = y0 + l;
-      float2 v = make_float2(0.f, 0.f);
-      if (isk) {
-        v.x = kern_val(hsq, M, x, y, z);
-      } else if (y < N && x < N) {
-        long g = x + (long)N * y;
-        if (D == 3) g += (long)N * N * z;
-        v = node_plane<D>(V[g], p);
+  const int nz_d = D == 3 ? N : 1, nz_k = D == 3 ? M : 1;
+  const long lines_d = 2L * N * nz_d, lines = lines_d + (long)M * nz_k;
+  const int wpb = blockDim.x >> 5;
+  for (long ln = (long)blockIdx.x * wpb + warp; ln < lines; ln += (long)gridDim.x * wpb) {
+    float2 v[E];
+    int p, y, z;
+    if (ln < lines_d) {
+      p = (int)(ln / ((long)N * nz_d));
+      const long r = ln % ((long)N * nz_d);
+      z = (int)(r / N);
+      y = (int)(r % N);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int x = lane + 32 * e;
+        v[e] = x < N ? node_plane<D>(V[x + (long)N * y + (D == 3 ? (long)N * N * z : 0)], p)
+                     : make_float2(0.f, 0.f);
       }
-      buf[l * ls + brev(x, logM)] = v;
-    }
-    __syncthreads();
-    fft_dit(buf, SGT_FFT_LINES, M, logM, tw);
-    float2 *Wp = W + p * plane;
-    const int ymax = isk ? M : N;
-    for (int e = threadIdx.x; e < SGT_FFT_LINES * M; e += blockDim.x) {
-      const int l = e / M, x = e % M, y = y0 + l;
-      if (y < ymax) {
-        long g = x + (long)M * y;
-        if (D == 3) g += (long)M * M * z;
-        Wp[g] = buf[l * ls + x];
-      }
-    }
-  }
-}
-
-// Load 8 adjacent-x lines along an axis with stride `stride` (in float2),
-// rows < lim valid (others zero), into buf in bit-reversed or natural order.
-__device__ __forceinline__ void load_lines(float2 *buf, const float2 *src,
-                                           long stride, int M, int logM,
-                                           int lim, bool bitrev) {
-  const int ls = SGT_LS(M);
-  for (int e = threadIdx.x; e < SGT_FFT_LINES * M; e += blockDim.x) {
-    const int l = e % SGT_FFT_LINES, t = e / SGT_FFT_LINES;
-    const float2 v = t < lim ? src[(long)t * stride + l] : make_float2(0.f, 0.f);
-    buf[l * ls + (bitrev ? brev(t, logM) : t)] = v;
-  }
-}
-__device__ __forceinline__ void store_lines(const float2 *buf, float2 *dst,
-                                            long stride, int M, int logM,
-                                            int lim, bool bitrev) {
-  const int ls = SGT_LS(M);
-  for (int e = threadIdx.x; e < SGT_FFT_LINES * lim; e += blockDim.x) {
-    const int l = e % SGT_FFT_LINES, t = e / SGT_FFT_LINES;
-    dst[(long)t * stride + l] = buf[l * ls + (bitrev ? brev(t, logM) : t)];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// d = 3, pass along y (forward: data planes z < N and kernel plane; inverse:
-// data planes z < N, keeping y < N).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SGT_THREADS)
-k_fft_mid_y(const SgtState *st, float2 *__restrict__ W, int inverse) {
-  extern __shared__ float2 sm[];
-  const int N = st->N, M = st->M, logM = st->logM;
-  const long plane = (long)M * M * M;
-  float2 *tw = sm, *buf = sm + 512;
-  fft_twiddles(tw, M);
-  const int nxb = M / SGT_FFT_LINES;
-  const int items_d = 2 * N * nxb;
-  const int items = inverse ? items_d : items_d + M * nxb;
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    int p, z, xb;
-    const bool isk = it >= items_d;
-    if (!isk) {
-      p = it / (N * nxb);
-      const int r = it % (N * nxb);
-      z = r / nxb;
-      xb = r % nxb;
     } else {
       p = 2;
-      const int r = it - items_d;
-      z = r / nxb;
-      xb = r % nxb;
+      const long r = ln - lines_d;
+      z = (int)(r / M);
+      y = (int)(r % M);
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = make_float2(kern_val(hsq, M, lane + 32 * e, y, z), 0.f);
     }
-    float2 *base = W + p * plane + (long)M * M * z + xb * SGT_FFT_LINES;
-    __syncthreads();
-    if (!inverse) {
-      load_lines(buf, base, M, M, logM, isk ? M : N, true);
-      __syncthreads();
-      fft_dit(buf, SGT_FFT_LINES, M, logM, tw);
-      store_lines(buf, base, M, M, logM, M, false);
-    } else {
-      load_lines(buf, base, M, M, logM, M, false);
-      __syncthreads();
-      fft_dif_inv(buf, SGT_FFT_LINES, M, logM, tw);
-      store_lines(buf, base, M, M, logM, N, true);
-    }
+    wfft_dif<LOGM>(v, tw);
+    float2 *row = W + p * plane + (long)M * y + (D == 3 ? (long)M * M * z : 0);
+#pragma unroll
+    for (int e = 0; e < E; e++) row[lane + 32 * e] = v[e];
   }
 }
 
-// ---------------------------------------------------------------------------
-// last axis (y for d = 2, z for d = 3): kernel spectrum, data forward,
-// pointwise product with Re(K^), inverse, keep positions < N.
-// ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(SGT_THREADS)
-k_fft_last(const SgtState *st, float2 *__restrict__ W) {
-  extern __shared__ float2 sm[];
-  const int N = st->N, M = st->M, logM = st->logM;
+k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
+  __shared__ float2 tw[512];
+  fft_twiddles(tw, st->M);
+  __syncthreads();
+#define CB(L) build_rows_body<D, L>(st, V, W, tw)
+  SGT_FFT_DISPATCH(st->logM, CB)
+#undef CB
+}
+
+// ---------------------------------------------------------------------------
+// column passes: 8 adjacent columns per CTA staged through shared memory.
+// MODE_LAST: last axis (y for d = 2, z for d = 3): kernel spectrum, data
+//            forward, product with Re(K^), inverse, keep positions < N.
+// MODE_MID_FWD / MODE_MID_INV: d = 3, axis y of the data planes z < N (and of
+//            the kernel plane on the forward pass).
+// ---------------------------------------------------------------------------
+#define MODE_LAST 0
+#define MODE_MID_FWD 1
+#define MODE_MID_INV 2
+
+template <int LOGM>
+__device__ __forceinline__ void stage_load(float2 *stg, const float2 *__restrict__ src, long stride,
+                                           int lim) {
+  constexpr int M = 1 << LOGM, LS = M + SGT_FFT_PAD;
+  for (int idx = threadIdx.x; idx < SGT_FFT_COLS * M; idx += blockDim.x) {
+    const int t = idx / SGT_FFT_COLS, c = idx % SGT_FFT_COLS;
+    stg[c * LS + t] = t < lim ? src[(long)t * stride + c] : make_float2(0.f, 0.f);
+  }
+}
+template <int LOGM>
+__device__ __forceinline__ void stage_store(const float2 *stg, float2 *__restrict__ dst, long stride,
+                                            int lim) {
+  constexpr int M = 1 << LOGM, LS = M + SGT_FFT_PAD;
+  for (int idx = threadIdx.x; idx < SGT_FFT_COLS * lim; idx += blockDim.x) {
+    const int t = idx / SGT_FFT_COLS, c = idx % SGT_FFT_COLS;
+    dst[(long)t * stride + c] = stg[c * LS + t];
+  }
+}
+
+template <int D, int MODE, int LOGM>
+__device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const float2 *tw,
+                          float2 *stg, float *kre) {
+  constexpr int M = 1 << LOGM, E = M / 32, LS = M + SGT_FFT_PAD;
+  const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long plane = D == 2 ? (long)M * M : (long)M * M * M;
-  const long stride = D == 2 ? (long)M : (long)M * M;
-  float2 *tw = sm, *bk = sm + 512, *bd = bk + SGT_FFT_LINES * SGT_LS(M);
-  fft_twiddles(tw, M);
-  const int nxb = M / SGT_FFT_LINES;
-  const int items = D == 2 ? nxb : nxb * M;
-  const int ls = SGT_LS(M);
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    const int xb = it % nxb, y = it / nxb;  // y used for d = 3
-    const long off = xb * SGT_FFT_LINES + (D == 3 ? (long)M * y : 0);
+  const int ncb = M / SGT_FFT_COLS;
+  // last pass: lines along y (d = 2, stride M) or z (d = 3, stride M^2)
+  const long stride = (MODE == MODE_LAST && D == 3) ? (long)M * M : (long)M;
+  long items;
+  if (MODE == MODE_LAST) items = D == 2 ? ncb : (long)ncb * M;  // d = 3: every y
+  else if (MODE == MODE_MID_FWD) items = (long)ncb * (2L * N + M);  // data z < N, kernel all z
+  else items = (long)ncb * 2L * N;
+  float2 v[E];
+  for (long it = blockIdx.x; it < items; it += gridDim.x) {
+    const int cb = (int)(it % ncb);
+    const long rest = it / ncb;
     __syncthreads();
-    load_lines(bk, W + 2 * plane + off, stride, M, logM, M, true);  // kernel plane
-    __syncthreads();
-    fft_dit(bk, SGT_FFT_LINES, M, logM, tw);
-    for (int p = 0; p < 2; p++) {
-      float2 *base = W + p * plane + off;
-      load_lines(bd, base, stride, M, logM, N, true);
+    if (MODE == MODE_LAST) {
+      const long off = (long)cb * SGT_FFT_COLS + (D == 3 ? (long)M * rest : 0);
+      // kernel spectrum of the 8 columns, real part kept
+      stage_load<LOGM>(stg, W + 2 * plane + off, stride, M);
       __syncthreads();
-      fft_dit(bd, SGT_FFT_LINES, M, logM, tw);
-      for (int e = threadIdx.x; e < SGT_FFT_LINES * M; e += blockDim.x) {
-        const int l = e / M, t = e % M;
-        const float kr = bk[l * ls + t].x;
-        const float2 v = bd[l * ls + t];
-        bd[l * ls + t] = make_float2(v.x * kr, v.y * kr);
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
+      wfft_dif<LOGM>(v, tw);
+#pragma unroll
+      for (int e = 0; e < E; e++) kre[warp * M + lane + 32 * e] = v[e].x;
+      for (int p = 0; p < 2; p++) {
+        float2 *base = W + p * plane + off;
+        __syncthreads();
+        stage_load<LOGM>(stg, base, stride, N);
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
+        wfft_dif<LOGM>(v, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const float kr = kre[warp * M + lane + 32 * e];
+          v[e] = make_float2(v[e].x * kr, v[e].y * kr);
+        }
+        wfft_dit_inv<LOGM>(v, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) stg[warp * LS + lane + 32 * e] = v[e];
+        __syncthreads();
+        stage_store<LOGM>(stg, base, stride, N);
       }
-      __syncthreads();
-      fft_dif_inv(bd, SGT_FFT_LINES, M, logM, tw);
-      store_lines(bd, base, stride, M, logM, N, true);
-      __syncthreads();
+    } else {
+      int p, z;
+      if (rest < 2L * N) {
+        p = (int)(rest / N);
+        z = (int)(rest % N);
+      } else {
+        p = 2;
+        z = (int)(rest - 2L * N);
+      }
+      float2 *base = W + p * plane + (long)M * M * z + (long)cb * SGT_FFT_COLS;
+      if (MODE == MODE_MID_FWD) {
+        stage_load<LOGM>(stg, base, M, p == 2 ? M : N);
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
+        wfft_dif<LOGM>(v, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) stg[warp * LS + lane + 32 * e] = v[e];
+        __syncthreads();
+        stage_store<LOGM>(stg, base, M, M);
+      } else {
+        stage_load<LOGM>(stg, base, M, M);
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
+        wfft_dit_inv<LOGM>(v, tw);
+#pragma unroll
+        for (int e = 0; e < E; e++) stg[warp * LS + lane + 32 * e] = v[e];
+        __syncthreads();
+        stage_store<LOGM>(stg, base, M, N);
+      }
     }
   }
 }
 
-// ---------------------------------------------------------------------------
-// final pass: inverse FFT along x of rows y (, z) < N, scale by 1/M^d and
-// write the potential grid (channels packed per node).
-// ---------------------------------------------------------------------------
-template <int D>
+template <int D, int MODE>
 __global__ void __launch_bounds__(SGT_THREADS)
-k_fft_final_x(const SgtState *st, const float2 *__restrict__ W,
-              typename Node<D>::T *__restrict__ Phi) {
+k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
   extern __shared__ float2 sm[];
-  const int N = st->N, M = st->M, logM = st->logM;
+  float2 *tw = sm;
+  float2 *stg = sm + 512;
+  float *kre = reinterpret_cast<float *>(stg + SGT_FFT_COLS * (st->M + SGT_FFT_PAD));
+  fft_twiddles(tw, st->M);
+  __syncthreads();
+#define CC(L) cols_body<D, MODE, L>(st, W, tw, stg, kre)
+  SGT_FFT_DISPATCH(st->logM, CC)
+#undef CC
+}
+
+// ---------------------------------------------------------------------------
+// final pass: inverse FFT along x of rows y (, z) < N, scale by 1/M^d, write
+// the potential grid (channels packed per node: plane 0 -> .xy, 1 -> .zw).
+// ---------------------------------------------------------------------------
+template <int D, int LOGM>
+__device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W,
+                                float2 *__restrict__ Phi2, const float2 *tw) {
+  constexpr int M = 1 << LOGM, E = M / 32;
+  const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long plane = D == 2 ? (long)M * M : (long)M * M * M;
-  float2 *tw = sm, *b0 = sm + 512, *b1 = b0 + SGT_FFT_LINES * SGT_LS(M);
-  fft_twiddles(tw, M);
-  const int nyb = (N + SGT_FFT_LINES - 1) / SGT_FFT_LINES;
-  const int items = nyb * (D == 3 ? N : 1);
-  const int ls = SGT_LS(M);
+  const long lines = 2L * N * (D == 3 ? N : 1);
+  const int wpb = blockDim.x >> 5;
   float inv = 1.0f / (float)M;
   inv = inv / (float)M;
   if (D == 3) inv = inv / (float)M;
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    const int y0 = (it % nyb) * SGT_FFT_LINES, z = it / nyb;
-    __syncthreads();
-    for (int e = threadIdx.x; e < SGT_FFT_LINES * M; e += blockDim.x) {
-      const int l = e / M, x = e % M, y = y0 + l;
-      float2 v0 = make_float2(0.f, 0.f), v1 = v0;
-      if (y < N) {
-        long g = x + (long)M * y + (D == 3 ? (long)M * M * z : 0);
-        v0 = W[g];
-        v1 = W[plane + g];
-      }
-      b0[l * ls + x] = v0;
-      b1[l * ls + x] = v1;
-    }
-    __syncthreads();
-    fft_dif_inv(b0, SGT_FFT_LINES, M, logM, tw);
-    fft_dif_inv(b1, SGT_FFT_LINES, M, logM, tw);
-    for (int e = threadIdx.x; e < SGT_FFT_LINES * N; e += blockDim.x) {
-      const int l = e / N, x = e % N, y = y0 + l;
-      if (y >= N) continue;
-      const float2 a = b0[l * ls + brev(x, logM)];
-      const float2 b = b1[l * ls + brev(x, logM)];
-      long g = x + (long)N * y + (D == 3 ? (long)N * N * z : 0);
-      Phi[g] = make_float4(a.x * inv, a.y * inv, b.x * inv, b.y * inv);
+  for (long ln = (long)blockIdx.x * wpb + warp; ln < lines; ln += (long)gridDim.x * wpb) {
+    const int p = (int)(ln % 2);
+    const long r = ln / 2;
+    const int y = (int)(r % N), z = D == 3 ? (int)(r / N) : 0;
+    const float2 *row = W + p * plane + (long)M * y + (D == 3 ? (long)M * M * z : 0);
+    float2 v[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = row[lane + 32 * e];
+    wfft_dit_inv<LOGM>(v, tw);
+    const long g0 = (long)N * y + (D == 3 ? (long)N * N * z : 0);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int x = lane + 32 * e;
+      if (x < N) Phi2[2 * (g0 + x) + p] = make_float2(v[e].x * inv, v[e].y * inv);
     }
   }
+}
+
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_fft_final_x(const SgtState *st, const float2 *__restrict__ W, typename Node<D>::T *__restrict__ Phi) {
+  __shared__ float2 tw[512];
+  fft_twiddles(tw, st->M);
+  __syncthreads();
+#define CF(L) final_rows_body<D, L>(st, W, reinterpret_cast<float2 *>(Phi), tw)
+  SGT_FFT_DISPATCH(st->logM, CF)
+#undef CF
+}
+
+// shared memory of a column pass for FFT length Mmax
+__host__ __device__ inline size_t fft_cols_smem(int Mmax) {
+  return sizeof(float2) * (512 + (size_t)SGT_FFT_COLS * (Mmax + SGT_FFT_PAD)) +
+         sizeof(float) * (size_t)SGT_FFT_COLS * Mmax;
 }

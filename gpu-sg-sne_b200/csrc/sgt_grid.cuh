@@ -386,7 +386,12 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
     if (D >= 3) o[2] = (ch.x / (td * td)) * T;
     for (int e = threadIdx.x; e < m * RD; e += blockDim.x) acc[e] = 0.f;
     __syncthreads();
-    for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
+    // each thread walks its own contiguous stretch of the chunk, so the lanes
+    // of a warp sit far apart in the (spatially ordered) chunk and their
+    // shared-memory atomics rarely meet on one node
+    const int per = (ch.z + blockDim.x - 1) / blockDim.x;
+    const int jb = ch.y + threadIdx.x * per, je = min(jb + per, ch.y + ch.z);
+    for (int j = jb; j < je; j++) {
       const float4 rec = sorted[j];
       int f[3];
       float w[3][4], ys[3];

@@ -79,10 +79,15 @@ typedef struct {
                        (0 = 512 for d <= 2, 128 for d = 3)              */
   int kl_every;     /* > 0: record the KL cost every kl_every iters     */
   uint64_t seed;    /* seed of the random Y0 when y_in is NULL          */
+  int relayout_every; /* > 0: relabel points along the Morton order of
+                         their grid cells every this many iterations
+                         (memory locality of the attractive term; results
+                         are returned in the caller's order).  0 = off    */
 } sgt_params;
 
 /* Fill *p with the reference defaults (d=2, lambda=1, alpha=12,
-   max_iter=1000, early_iter=250, h=-1, format=SGT_FORMAT_COO, ng=50). */
+   max_iter=1000, early_iter=250, h=-1, format=SGT_FORMAT_COO, ng=50);
+   relayout_every = 0. */
 void sgt_params_default(sgt_params *p);
 
 typedef struct sgt_ctx sgt_ctx;

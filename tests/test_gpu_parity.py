@@ -277,3 +277,28 @@ def test_invalid_csr_rejected(torch, ctx):
     with pytest.raises(S.SgtError) as e:
         S.Job(ctx, p, rp, col, np.ones(3, np.float32), device_mem=False)
     assert e.value.status == 1
+
+
+def test_relayout_is_transparent(torch, ctx):
+    """Locality relabelling every 10 iterations against none: the caller sees
+    the same embedding in the same point order (per-row sums are
+    bit-identical; only the order of the FP32 scatter atomics differs)."""
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=4000, k=12, seed=9)
+    n = len(rp) - 1
+    Y0 = (np.random.default_rng(4).standard_normal((n, 2)) * 5).astype(np.float32)
+    out = {}
+    for every in (0, 10):
+        p = S.default_params(d=2, format=S.FORMAT_CSR)
+        p.relayout_every = every
+        job = S.Job(ctx, p, rp, col, val.astype(np.float32), device_mem=False)
+        job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+        job.run(35)
+        out[every] = job.get_y(np.empty((n, 2), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        # a second run from the same start after relabelling still maps back
+        job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+        job.run(35)
+        again = job.get_y(np.empty((n, 2), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        assert rel(again, out[every]) <= 1e-4
+        job.close()
+    assert rel(out[10], out[0]) <= 1e-4
