@@ -220,6 +220,7 @@ def run_ours(args, rank, world, local, dist):
     t_setup = time.time() - t_setup
     p = S.default_params(d=d, format=S.FORMAT_CSR, max_iter=1000, early_iter=250, h=0.7)
     p.lambda_ = 10.0
+    p.relayout_every = args.relayout
     Ystate = expanded_state(X, d, args.spread, args.seed)
     del X
 
@@ -305,6 +306,7 @@ def run_ours(args, rank, world, local, dist):
             "config": {"workload": WORKLOAD, "n": n, "d": d, "nnz": nnz, "format": "csr",
                        "parallelism": f"replicas x{world}", "grid_points": info.grid_points,
                        "h_eff": round(info.h_eff, 5), "row_group": info.row_group,
+                       "relayout_every": args.relayout,
                        "row_group_tune_ms": [round(x, 4) for x in info.tune_ms],
                        "timed_state":
                        f"fixed expanded embedding (std {args.spread}), {args.warmup} warm-up steps",
@@ -385,6 +387,8 @@ def main():
     ap.add_argument("--spread", type=float, default=60.0)
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--relayout", type=int, default=0,
+                    help="relabel points along the cell Morton order every R iterations (0 = off)")
     ap.add_argument("--no-full-run", dest="full_run", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     args = ap.parse_args()

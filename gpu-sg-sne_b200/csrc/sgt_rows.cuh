@@ -33,7 +33,7 @@ __device__ __forceinline__ void attr_term(const typename Vec<D>::T &yi,
     df[k] = comp<D>(yi, k) - comp<D>(yj, k);
     dist += df[k] * df[k];
   }
-  const float pq = p / (1.0f + dist);
+  const float pq = __fdividef(p, 1.0f + dist);  // <= 2 ulp; p/(1+d^2) of the reference
 #pragma unroll
   for (int k = 0; k < D; k++) acc[k] += pq * df[k];
 }
