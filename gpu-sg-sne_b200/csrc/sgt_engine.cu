@@ -1484,3 +1484,145 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   sgt_job_destroy(J);
   return st;
 }
+
+// ---------------------------------------------------------------------------
+// Interpolated repulsion without device allocation.
+//
+// For callers that may not allocate device memory at all: applications whose
+// own pool allocator has reserved the whole device (a cudaMalloc would fail
+// or fragment their pool), and latency-sensitive loops where a cudaMalloc /
+// cudaFree pair would stall on device synchronisation.  All scratch lives in
+// one file-scope __device__ array, held by every GPU that loads this library
+// until the process exits.  Limits: n <= SGT_NA_MAX_N points, d = 1 or 2,
+// grids up to 128 points per axis in 2-D (512 in 1-D).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+constexpr int SGT_NA_MAX_N = 32768;
+constexpr int SGT_NA_MAX_GRID_2D = 128;   // points per axis -> FFT length 256
+constexpr int SGT_NA_MMAX_2D = 256;
+constexpr int SGT_NA_MMAX_1D = 1024;
+constexpr int SGT_NA_PARTS = 4096;        // per-block partials of the reductions
+constexpr int SGT_NA_CHUNKS = SGT_NA_MAX_N / 1024 + SGT_HIST_MAX + 16;
+constexpr size_t na_al(size_t b) { return (b + 255) & ~(size_t)255; }
+// byte offsets of every buffer inside the array
+constexpr size_t NA_Y = 0;
+constexpr size_t NA_YNEXT = NA_Y + na_al((size_t)SGT_NA_MAX_N * 2 * 4);
+constexpr size_t NA_FREP = NA_YNEXT + na_al((size_t)SGT_NA_MAX_N * 2 * 4);
+constexpr size_t NA_SORTED = NA_FREP + na_al((size_t)SGT_NA_MAX_N * 2 * 4);
+constexpr size_t NA_NODES = (size_t)SGT_NA_MAX_GRID_2D * SGT_NA_MAX_GRID_2D;  // >= 512 (1-D)
+constexpr size_t NA_V = NA_SORTED + na_al((size_t)SGT_NA_MAX_N * 16);
+constexpr size_t NA_PHI = NA_V + na_al(NA_NODES * 16);
+constexpr size_t NA_W = NA_PHI + na_al(NA_NODES * 16);
+constexpr size_t NA_TILES = NA_W + na_al((size_t)3 * SGT_NA_MMAX_2D * SGT_NA_MMAX_2D * 8);
+constexpr size_t NA_CURSOR = NA_TILES + na_al((size_t)SGT_HIST_MAX * 4);
+constexpr size_t NA_CHUNKS = NA_CURSOR + na_al((size_t)SGT_HIST_MAX * 4);
+constexpr size_t NA_PMIN = NA_CHUNKS + na_al((size_t)SGT_NA_CHUNKS * 16);
+constexpr size_t NA_PMAX = NA_PMIN + na_al((size_t)SGT_NA_PARTS * 16);
+constexpr size_t NA_PSUM = NA_PMAX + na_al((size_t)SGT_NA_PARTS * 16);
+constexpr size_t NA_PZ = NA_PSUM + na_al((size_t)SGT_NA_PARTS * 4 * 8);
+constexpr size_t NA_STATE = NA_PZ + na_al((size_t)SGT_NA_PARTS * 8);
+constexpr size_t NA_BYTES = NA_STATE + na_al(sizeof(SgtState));
+static_assert(NA_BYTES < 8u << 20, "no-alloc scratch stays a few MB");
+}  // namespace
+
+// The scratch itself.  In host code this name is only a host-side stand-in;
+// kernels receive the device address obtained with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_sgt_noalloc_scratch[NA_BYTES];
+
+static std::mutex g_na_mutex;
+static void *g_na_addr[64];  // device address of the scratch, per device
+
+static sgt_status noalloc_scratch(sgt_ctx *ctx, unsigned char **out) {
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, SGT_ERR_UNSUPPORTED, "device index >= 64");
+  if (!g_na_addr[ctx->device]) {  // once per device, with that device current
+    void *p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_sgt_noalloc_scratch));
+    g_na_addr[ctx->device] = p;
+  }
+  *out = (unsigned char *)g_na_addr[ctx->device];
+  return SGT_OK;
+}
+
+extern "C" sgt_status sgt_repulsive_noalloc(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
+                                            const float *y, int layout, float *f, double *zeta,
+                                            int *grid_points, float *h_eff) {
+  if (!ctx || !y || !f) return SGT_ERR_INVALID_ARG;
+  if (n < 2 || n > SGT_NA_MAX_N)
+    return fail(ctx, SGT_ERR_INVALID_ARG,
+                "sgt_repulsive_noalloc: n must be in [2, " + std::to_string(SGT_NA_MAX_N) + "]");
+  if (d < 1 || d > 2)
+    return fail(ctx, SGT_ERR_INVALID_ARG, "sgt_repulsive_noalloc: d must be 1 or 2");
+  if (ng_fixed > 0 && d == 2 && sgt_best_grid_size(ng_fixed) + 2 > SGT_NA_MAX_GRID_2D)
+    return fail(ctx, SGT_ERR_INVALID_ARG,
+                "sgt_repulsive_noalloc: fixed grid larger than 128 points per axis");
+  CK(cudaSetDevice(ctx->device));
+  unsigned char *base = nullptr;
+  CKS(noalloc_scratch(ctx, &base));
+  cudaStream_t s = ctx->stream;
+  // a job view over the static scratch (host stack only)
+  sgt_job J;
+  J.ctx = ctx;
+  sgt_params_default(&J.p);
+  J.p.d = d;
+  J.p.format = SGT_FORMAT_CSR;
+  J.n = n;
+  J.d = d;
+  J.S = d;
+  J.G = 8;
+  J.p.grid_mode = ng_fixed > 0 ? SGT_GRID_FIXED : SGT_GRID_H;
+  fill_jp(&J);
+  J.jp.grid_mode = J.p.grid_mode;
+  J.jp.n1_fixed = sgt_best_grid_size(ng_fixed > 0 ? ng_fixed : 50);
+  J.jp.h = h > 0 ? h : (d == 1 ? 0.5f : 0.7f);
+  J.mmax = d == 1 ? SGT_NA_MMAX_1D : SGT_NA_MMAX_2D;
+  J.nmax = d == 1 ? 512 : SGT_NA_MAX_GRID_2D;
+  J.jp.mmax = J.mmax;
+  J.jp.tile_cap = SGT_HIST_MAX;
+  J.jp.chunk_cap = SGT_NA_CHUNKS;
+  J.Y = (float *)(base + NA_Y);
+  J.Ynext = (float *)(base + NA_YNEXT);
+  J.Frep = (float *)(base + NA_FREP);
+  J.sorted = (float4 *)(base + NA_SORTED);
+  J.V = (float *)(base + NA_V);
+  J.Phi = (float *)(base + NA_PHI);
+  J.W = (float2 *)(base + NA_W);
+  J.tile_count = (int *)(base + NA_TILES);
+  J.cursor = (int *)(base + NA_CURSOR);
+  J.chunks = (int4 *)(base + NA_CHUNKS);
+  J.part_min = (float4 *)(base + NA_PMIN);
+  J.part_max = (float4 *)(base + NA_PMAX);
+  J.part_sum = (double *)(base + NA_PSUM);
+  J.part_z = (double *)(base + NA_PZ);
+  J.st = (SgtState *)(base + NA_STATE);
+  sgt_status stt = d == 1 ? job_shapes<1>(&J) : job_shapes<2>(&J);
+  if (stt != SGT_OK) return stt;
+  if (std::max(std::max(J.nb_pts, J.nb_s2g), J.nb_g2s) > SGT_NA_PARTS)
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "sgt_repulsive_noalloc: too many blocks for the partials");
+  // the array keeps the previous call's contents: clear what starts at zero
+  CK(cudaMemsetAsync(J.st, 0, sizeof(SgtState), s));
+  CK(cudaMemsetAsync(J.tile_count, 0, sizeof(int) * SGT_HIST_MAX, s));
+  CKS(pack_y(&J, y, layout, J.Ynext, s));
+  CKS(init_stats(&J, s, 0));
+  if (d == 1) CKS(enqueue_repulsion<1>(&J, s));
+  else CKS(enqueue_repulsion<2>(&J, s));
+  const int nb = grid_blocks(ctx->nsm, 4);
+  const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+  if (d == 1) k_unpack_divz<1><<<nb, SGT_THREADS, 0, s>>>((const float *)J.Frep, n, dm, J.st, f);
+  else k_unpack_divz<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)J.Frep, n, dm, J.st, f);
+  CK(cudaGetLastError());
+  SgtState hs;
+  CK(cudaMemcpyAsync(&hs, J.st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (hs.grid_clamped)
+    return fail(ctx, SGT_ERR_INVALID_ARG,
+                "sgt_repulsive_noalloc: the embedding needs a grid above 128 points per axis; "
+                "use sgt_repulsive");
+  if (zeta) *zeta = hs.Z;
+  if (grid_points) *grid_points = hs.N;
+  if (h_eff) *h_eff = hs.h_eff;
+  if (hs.error & SGT_EFLAG_NONFINITE) return fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates");
+  return SGT_OK;
+}

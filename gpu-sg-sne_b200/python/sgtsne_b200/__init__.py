@@ -70,6 +70,8 @@ SIGNATURES = {
     "sgt_attractive": (_i, [_vp, _i, _i, _i, _l, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "sgt_repulsive": (_i, [_vp, _i, _i, _f, _i, _vp, _i, _vp, C.POINTER(_d),
                            C.POINTER(_i), C.POINTER(_f)]),
+    "sgt_repulsive_noalloc": (_i, [_vp, _i, _i, _f, _i, _vp, _i, _vp, C.POINTER(_d),
+                                   C.POINTER(_i), C.POINTER(_f)]),
     "sgt_bins": (_i, [_vp, _i, _i, _f, _i, _vp, _i, _vp, C.POINTER(_i)]),
     "sgt_last_grids": (_i, [_vp, _vp, _vp]),
     "sgt_best_grid_size": (_i, [_i]),
@@ -164,6 +166,16 @@ class Context:
         self.check(self.lib.sgt_repulsive(self.h, n, d, float(h), int(ng_fixed), _ptr(y), layout,
                                           _ptr(f), C.byref(z), C.byref(gp), C.byref(he)),
                    "repulsive")
+        return z.value, gp.value, he.value
+
+    def repulsive_noalloc(self, n, d, h, ng_fixed, y, layout, f):
+        """sgt_repulsive_noalloc: the repulsion with no device allocation."""
+        z = C.c_double()
+        gp = C.c_int()
+        he = C.c_float()
+        self.check(self.lib.sgt_repulsive_noalloc(self.h, n, d, float(h), int(ng_fixed), _ptr(y),
+                                                  layout, _ptr(f), C.byref(z), C.byref(gp),
+                                                  C.byref(he)), "repulsive_noalloc")
         return z.value, gp.value, he.value
 
     def bins(self, n, d, h, ng_fixed, y, layout, out):

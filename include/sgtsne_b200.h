@@ -172,6 +172,27 @@ sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
                          const float *y, int layout, float *f, double *zeta,
                          int *grid_points, float *h_eff);
 
+/* sgt_repulsive without any device allocation.  No counterpart in the
+   reference: it exists for callers that must not allocate device memory,
+   e.g. an application whose own pool allocator has reserved the whole GPU
+   (a cudaMalloc would fail or fragment that pool) or a latency-sensitive
+   loop where a cudaMalloc/cudaFree pair would stall on synchronisation.
+   Same arguments and results as sgt_repulsive; all scratch lives in one
+   fixed array of about 4 MB inside this library, which every GPU that loads
+   the library holds until the process exits.
+   Limits: 2 <= n <= 32768, d = 1 or 2, a grid of at most 128 points per axis
+   in 2-D (512 in 1-D); anything larger is rejected with SGT_ERR_INVALID_ARG
+   and a message (an embedding wider than the limit is detected after the
+   work ran, its forces are not written to be used).
+   The first call on a device looks up the array's device address
+   (cudaGetSymbolAddress) and must come before any stream capture.  Calls
+   share the array: calls that overlap on the GPU (other streams, other host
+   threads on the same device) race and must be serialised by the caller. */
+sgt_status sgt_repulsive_noalloc(sgt_ctx *ctx, int n, int d, float h,
+                                 int ng_fixed, const float *y, int layout,
+                                 float *f, double *zeta, int *grid_points,
+                                 float *h_eff);
+
 /* The integer part of the repulsion: per point and dim the floor bin of the
    scaled coordinate (CU/nuconv.cu:9-36 + CU/gridding.cu:159-167), and the
    grid size.  bins: device uint32 n*d point-major. */
