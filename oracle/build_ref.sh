@@ -1,0 +1,21 @@
+#!/bin/bash
+# Compiles the reference's own CUDA sources, where they lie under
+# /root/reference, with the test-only harnesses of oracle/ref_harness into
+# oracle/_ref/ (git-ignored; the built .so files travel with the repository
+# to the GPU box).  Used only to produce golden vectors of the reference.
+set -e
+HERE="$(cd "$(dirname "$0")" && pwd)"
+REF=/root/reference/code/cuda
+OUT="$HERE/_ref"
+[ -d "$REF" ] || { echo "reference tree not mounted; nothing to build"; exit 0; }
+mkdir -p "$OUT"
+FLAGS="-std=c++14 -O2 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -shared -w"
+HYB="$REF/SG-tSNE-HYB/sgtsnepi/src"
+nvcc $FLAGS -I"$HYB/cuda" -I"$HYB" -o "$OUT/libref_hyb.so" "$HERE/ref_harness/ref_hyb.cu" \
+  "$HYB/cuda/Frep.cu" "$HYB/cuda/nuconv.cu" "$HYB/cuda/gridding.cu" \
+  "$HYB/cuda/non_periodic_convF.cu" "$HYB/cuda/non_periodic_convD.cu" -lcufft
+CU="$REF/SG-tSNE-CUDA/src"
+nvcc $FLAGS -I"$CU" -o "$OUT/libref_cu.so" "$HERE/ref_harness/ref_cu.cu" \
+  "$CU/pq.cu" "$CU/Frep.cu" "$CU/nuconv.cu" "$CU/gridding.cu" \
+  "$CU/non_periodic_convF.cu" "$CU/non_periodic_convD.cu" "$CU/utils.cu" -lcufft
+echo "built $OUT/libref_hyb.so $OUT/libref_cu.so"
