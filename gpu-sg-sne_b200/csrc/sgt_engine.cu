@@ -70,7 +70,7 @@ struct sgt_job {
   double *part_sum = nullptr, *part_z = nullptr, *part_kl = nullptr;
   SgtState *st = nullptr;
   SgtState *st_host = nullptr;
-  int nb_pts = 0, nb_s2g = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0, nb_part = 0;
+  int nb_pts = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0, nb_part = 0;
   size_t smem_s2g = 0, smem_fft1 = 0, smem_fft2 = 0;
   cudaGraphExec_t gexec = nullptr;
   std::vector<void *> allocs;
@@ -99,12 +99,17 @@ static sgt_status fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) {
     if (s_ != SGT_OK) return s_;                                              \
   } while (0)
 
+// Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
+// context's stream from the device's default pool): creating or retiring a
+// job never waits for work on other streams, which cudaFree would (it
+// synchronises the device).  Jobs of one context share its stream, so
+// every use of a buffer is ordered between its allocation and its free.
 template <typename T>
 static sgt_status jalloc(sgt_job *J, T **ptr, size_t count) {
   sgt_ctx *ctx = J->ctx;
   void *p = nullptr;
   if (count == 0) count = 1;
-  CK(cudaMalloc(&p, count * sizeof(T)));
+  CK(cudaMallocAsync(&p, count * sizeof(T), ctx->stream));
   J->allocs.push_back(p);
   *ptr = (T *)p;
   return SGT_OK;
@@ -200,6 +205,13 @@ void sgt_destroy(sgt_ctx *ctx) {
 sgt_status sgt_set_stream(sgt_ctx *ctx, void *stream) {
   if (!ctx) return SGT_ERR_INVALID_ARG;
   CK(cudaSetDevice(ctx->device));
+  // work queued so far (and the stream-ordered frees of jobs destroyed
+  // later on the new stream) must not overlap: drain the old stream
+  if (ctx->stream) CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->scratch) {
+    sgt_job_destroy(ctx->scratch);
+    ctx->scratch = nullptr;
+  }
   if (ctx->own_stream && ctx->stream) CK(cudaStreamDestroy(ctx->stream));
   if (stream) {
     ctx->stream = (cudaStream_t)stream;
@@ -207,10 +219,6 @@ sgt_status sgt_set_stream(sgt_ctx *ctx, void *stream) {
   } else {
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     ctx->own_stream = true;
-  }
-  if (ctx->scratch) {
-    sgt_job_destroy(ctx->scratch);
-    ctx->scratch = nullptr;
   }
   return SGT_OK;
 }
@@ -257,6 +265,8 @@ static sgt_status job_shapes(sgt_job *J) {
   CK(cudaFuncSetAttribute(k_s2g<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_s2g));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g<D>, SGT_THREADS, J->smem_s2g));
   J->nb_s2g = grid_blocks(nsm, occ);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g_cell<D>, SGT_THREADS, 0));
+  J->nb_s2gc = grid_blocks(nsm, occ);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2s<D>, SGT_THREADS, 0));
   J->nb_g2s = grid_blocks(nsm, occ);
   const int M = J->mmax;
@@ -283,6 +293,19 @@ static sgt_status job_shapes(sgt_job *J) {
     default: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 32, true>, SGT_THREADS, 0)); break;
   }
   J->nb_row = grid_blocks(nsm, occ);
+  // small embeddings launch no more blocks than there is work for: idle
+  // blocks only take scheduling slots from the jobs that share the GPU
+  const int cap = (int)std::max(1L, ((long)J->n + 255) / 256);
+  J->nb_pts = std::min(J->nb_pts, cap);
+  J->nb_s2g = std::min(J->nb_s2g, cap);
+  J->nb_s2gc = std::min(J->nb_s2gc, cap);
+  J->nb_g2s = std::min(J->nb_g2s, cap);
+  J->nb_row = std::min(J->nb_row, cap);
+  if constexpr (D == 2) {  // lines of the largest grid this job can take
+    const int lines_rows = 2 * J->nmax + J->mmax, lines_cols = J->mmax / SGT_FFT_COLS;
+    J->nb_fft_rows = std::min(J->nb_fft_rows, (lines_rows + 7) / 8);
+    J->nb_fft = std::min(J->nb_fft, std::max(1, lines_cols));
+  }
   J->nb_part = std::max(std::max(J->nb_pts, J->nb_row), std::max(J->nb_g2s, J->nb_s2g));
   // the fused CSR row kernel launches ceil(n * G / 256) blocks, G <= 32
   J->nb_part = std::max(J->nb_part, (int)(((long)J->n * 32 + SGT_THREADS - 1) / SGT_THREADS));
@@ -326,7 +349,7 @@ static sgt_status job_alloc(sgt_job *J) {
   J->jp.mmax = M;
   J->jp.tile_cap = SGT_HIST_MAX;
   CKS(jalloc(J, &J->st, 1));
-  CK(cudaMallocHost((void **)&J->st_host, sizeof(SgtState)));
+  J->st_host = new SgtState();
   CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, ctx->stream));
   CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), ctx->stream));
   return SGT_OK;
@@ -402,8 +425,9 @@ static sgt_status enqueue_g2g(sgt_job *J, cudaStream_t s) {
   return SGT_OK;
 }
 
+// ev (optional): events recorded after the binning, S2G and G2G stages
 template <int D>
-static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s) {
+static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   typedef typename Node<D>::T NT;
@@ -413,8 +437,13 @@ static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s) {
   k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
   k_bin_scatter<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, n, J->st, J->cursor,
                                                      J->sorted);
+  if (ev) CK(cudaEventRecord(ev[1], s));
+  // tile mode and cell mode: the kernel of the other mode returns at once
   k_s2g<D><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+  k_s2g_cell<D><<<J->nb_s2gc, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+  if (ev) CK(cudaEventRecord(ev[2], s));
   CKS(enqueue_g2g<D>(J, s));
+  if (ev) CK(cudaEventRecord(ev[3], s));
   k_g2s<D><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi,
                                              (VT *)J->Frep, J->part_z, n);
   CK(cudaGetLastError());
@@ -499,6 +528,11 @@ static sgt_status pack_y(sgt_job *J, const float *src, int layout, float *dst, c
   }
   CK(cudaGetLastError());
   return SGT_OK;
+}
+
+__global__ void k_fill(float *__restrict__ p, long count, float v) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x)
+    p[i] = v;
 }
 
 template <int D>
@@ -603,8 +637,8 @@ static sgt_status tune_group_d(sgt_job *J) {
   const size_t np = (size_t)J->n * J->S;
   float *buf = nullptr;
   SgtState *tst = nullptr;
-  CK(cudaMalloc(&buf, sizeof(float) * np * 4));
-  CK(cudaMalloc(&tst, sizeof(SgtState)));
+  CK(cudaMallocAsync(&buf, sizeof(float) * np * 4, s));
+  CK(cudaMallocAsync(&tst, sizeof(SgtState), s));
   CK(cudaMemsetAsync(buf, 0, sizeof(float) * np * 4, s));
   CK(cudaMemsetAsync(J->Frep, 0, sizeof(float) * np, s));
   SgtState h;
@@ -625,8 +659,8 @@ static sgt_status tune_group_d(sgt_job *J) {
   cudaError_t e = cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(buf);
-  cudaFree(tst);
+  cudaFreeAsync(buf, s);
+  cudaFreeAsync(tst, s);
   CK(e);
   CK(cudaGetLastError());
   int best = 0;
@@ -770,13 +804,13 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   (void)need_host;
   if (mem_is_device && params->format != SGT_FORMAT_HYBRID) {
     int *bad = nullptr;
-    CK(cudaMalloc(&bad, sizeof(int)));
+    CK(cudaMallocAsync(&bad, sizeof(int), s));
     CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
     k_validate_csr<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(n, rowptr, col, bad);
     int hb = 0;
     CK(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    cudaFree(bad);
+    cudaFreeAsync(bad, s);
     if (hb) return fail(ctx, SGT_ERR_INVALID_ARG, "malformed CSR (rowptr order or column range)");
   }
   sgt_job *J = new sgt_job();
@@ -824,8 +858,8 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
       dcol = (int *)col;
       dval = (float *)val;
     } else {
-      if (cudaMalloc(&dcol, sizeof(int) * nnz) != cudaSuccess ||
-          cudaMalloc(&dval, sizeof(float) * nnz) != cudaSuccess)
+      if (cudaMallocAsync(&dcol, sizeof(int) * nnz, s) != cudaSuccess ||
+          cudaMallocAsync(&dval, sizeof(float) * nnz, s) != cudaSuccess)
         return bail(fail(ctx, SGT_ERR_NO_MEMORY, "staging P"));
       cudaMemcpyAsync(dcol, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, s);
       cudaMemcpyAsync(dval, val, sizeof(float) * nnz, cudaMemcpyHostToDevice, s);
@@ -844,9 +878,8 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
     }
     if (cudaGetLastError() != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "packing P"));
     if (!mem_is_device) {
-      cudaStreamSynchronize(s);
-      cudaFree(dcol);
-      cudaFree(dval);
+      cudaFreeAsync(dcol, s);
+      cudaFreeAsync(dval, s);
     }
   } else {  // hybrid: host split like CU/prepareMatrix.cu:55-97
     const int *hc = mem_is_device ? hcol.data() : col;
@@ -890,8 +923,11 @@ void sgt_job_destroy(sgt_job *J) {
   if (!J) return;
   if (J->ctx) cudaSetDevice(J->ctx->device);
   if (J->gexec) cudaGraphExecDestroy(J->gexec);
-  for (void *p : J->allocs) cudaFree(p);
-  if (J->st_host) cudaFreeHost(J->st_host);
+  if (J->ctx) {
+    cudaStream_t s = J->ctx->stream;
+    for (void *p : J->allocs) cudaFreeAsync(p, s);
+  }
+  delete J->st_host;
   delete J;
 }
 
@@ -904,7 +940,7 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
   const float *src = y;
   float *staging = nullptr;
   if (!mem_is_device) {
-    CK(cudaMalloc(&staging, bytes));
+    CK(cudaMallocAsync(&staging, bytes, s));
     CK(cudaMemcpyAsync(staging, y, bytes, cudaMemcpyHostToDevice, s));
     src = staging;
   }
@@ -922,18 +958,14 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
     CKS(pack_y(J, src, layout, J->Ynext, s));
   }
   CK(cudaMemsetAsync(J->uY, 0, sizeof(float) * (size_t)J->n * J->S, s));
-  {
-    std::vector<float> ones((size_t)J->n * J->S, 1.0f);
-    CK(cudaMemcpyAsync(J->gains, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));
-  }
+  k_fill<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(J->gains, (long)J->n * J->S, 1.0f);
   CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
   CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, s));
   CKS(init_stats(J, s, 1));
   J->host_iter = 0;
   if (staging) {
     CK(cudaStreamSynchronize(s));
-    CK(cudaFree(staging));
+    CK(cudaFreeAsync(staging, s));
   }
   return SGT_OK;
 }
@@ -987,7 +1019,7 @@ sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, in
   const size_t bytes = sizeof(float) * (size_t)J->n * J->d;
   float *dst = y, *staging = nullptr;
   if (!mem_is_device) {
-    CK(cudaMalloc(&staging, bytes));
+    CK(cudaMallocAsync(&staging, bytes, s));
     dst = staging;
   }
   const int nb = grid_blocks(ctx->nsm, 4);
@@ -1001,7 +1033,7 @@ sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, in
   if (staging) {
     CK(cudaMemcpyAsync(y, staging, bytes, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    CK(cudaFree(staging));
+    CK(cudaFreeAsync(staging, s));
   } else {
     CK(cudaStreamSynchronize(s));
   }
@@ -1065,50 +1097,13 @@ sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
   cudaStream_t s = ctx->stream;
   cudaEvent_t ev[6];
   for (int i = 0; i < 6; i++) CK(cudaEventCreate(&ev[i]));
-  typedef void (*fn_t)(sgt_job *, cudaStream_t);
   for (int it = 0; it < iters; it++) {
     // same kernels as the graph, bracketed per stage
     CK(cudaEventRecord(ev[0], s));
     switch (J->d) {
-      case 1: {
-        typedef Vec<1>::T VT; typedef Node<1>::T NT;
-        k_bin_count<1><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n, J->st, J->tile_count, (NT *)J->V, 1);
-        k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
-        k_bin_scatter<1><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, J->n, J->st, J->cursor, J->sorted);
-        CK(cudaEventRecord(ev[1], s));
-        k_s2g<1><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
-        CK(cudaEventRecord(ev[2], s));
-        CKS(enqueue_g2g<1>(J, s));
-        CK(cudaEventRecord(ev[3], s));
-        k_g2s<1><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
-        break;
-      }
-      case 2: {
-        typedef Vec<2>::T VT; typedef Node<2>::T NT;
-        k_bin_count<2><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n, J->st, J->tile_count, (NT *)J->V, 1);
-        k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
-        k_bin_scatter<2><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, J->n, J->st, J->cursor, J->sorted);
-        CK(cudaEventRecord(ev[1], s));
-        k_s2g<2><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
-        CK(cudaEventRecord(ev[2], s));
-        CKS(enqueue_g2g<2>(J, s));
-        CK(cudaEventRecord(ev[3], s));
-        k_g2s<2><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
-        break;
-      }
-      default: {
-        typedef Vec<3>::T VT; typedef Node<3>::T NT;
-        k_bin_count<3><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n, J->st, J->tile_count, (NT *)J->V, 1);
-        k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
-        k_bin_scatter<3><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, J->n, J->st, J->cursor, J->sorted);
-        CK(cudaEventRecord(ev[1], s));
-        k_s2g<3><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
-        CK(cudaEventRecord(ev[2], s));
-        CKS(enqueue_g2g<3>(J, s));
-        CK(cudaEventRecord(ev[3], s));
-        k_g2s<3><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n);
-        break;
-      }
+      case 1: CKS(enqueue_repulsion<1>(J, s, ev)); break;
+      case 2: CKS(enqueue_repulsion<2>(J, s, ev)); break;
+      default: CKS(enqueue_repulsion<3>(J, s, ev)); break;
     }
     CK(cudaEventRecord(ev[4], s));
     switch (J->d * 100 + J->G) {
@@ -1235,7 +1230,7 @@ sgt_status sgt_attractive(sgt_ctx *ctx, int format, int n, int d, long nnz, cons
   tmp.S = d == 3 ? 4 : d;
   const int S = tmp.S;
   sgt_status st = SGT_OK;
-  auto cleanup = [&]() { for (void *q : tmp.allocs) cudaFree(q); tmp.allocs.clear(); };
+  auto cleanup = [&]() { for (void *q : tmp.allocs) cudaFreeAsync(q, s); tmp.allocs.clear(); };
   float *Yp = nullptr, *Fp = nullptr;
   if ((st = jalloc(&tmp, &Yp, (size_t)n * S)) != SGT_OK || (st = jalloc(&tmp, &Fp, (size_t)n * S)) != SGT_OK) {
     cleanup();
@@ -1330,7 +1325,7 @@ sgt_status sgt_kl(sgt_ctx *ctx, int n, int d, long nnz, const int *rowptr, const
   tmp.n = n;
   tmp.S = d == 3 ? 4 : d;
   sgt_status st;
-  auto cleanup = [&]() { for (void *q : tmp.allocs) cudaFree(q); tmp.allocs.clear(); };
+  auto cleanup = [&]() { for (void *q : tmp.allocs) cudaFreeAsync(q, s); tmp.allocs.clear(); };
   float *Yp;
   int2 *pairs;
   SgtState *sd;
@@ -1428,8 +1423,8 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   if (p.lambda != 1.0f) {
     int *drp = nullptr;
     float *dv = nullptr;
-    CK(cudaMalloc(&drp, sizeof(int) * (n + 1)));
-    CK(cudaMalloc(&dv, sizeof(float) * nnz));
+    CK(cudaMallocAsync(&drp, sizeof(int) * (n + 1), s));
+    CK(cudaMallocAsync(&dv, sizeof(float) * nnz, s));
     CK(cudaMemcpyAsync(drp, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dv, v.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
     sgt_status ls = sgt_lambda_bisect(ctx, n, drp, dv, p.lambda, p.lambda_dist, nullptr);
@@ -1437,8 +1432,8 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
       CK(cudaMemcpyAsync(v.data(), dv, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
     }
-    cudaFree(drp);
-    cudaFree(dv);
+    cudaFreeAsync(drp, s);
+    cudaFreeAsync(dv, s);
     if (ls != SGT_OK) return ls;
     if (p.drop_leaf)
       for (int r = 0; r < n; r++)

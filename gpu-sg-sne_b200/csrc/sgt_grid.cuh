@@ -17,6 +17,8 @@
 #pragma once
 #include "sgt_common.cuh"
 
+#define SGT_HIST_MAX 4096  // tiles held in shared memory by the binning kernels
+
 // ---------------------------------------------------------------------------
 // Grid decision from the stats of the coordinates that the next kernels bin.
 // minv/maxv are per-dim min/max of Ynext, sums its per-dim sums; the
@@ -70,8 +72,15 @@ __device__ void sgt_finalize_grid(SgtState *st, const SgtJobParams &jp,
   st->logM = logM;
   st->scale = (float)(unsigned)(N - 3);
   st->h_eff = __fdiv_rn(maxy, (float)(n1 - 1) - 1.1920928955078125e-7f);
-  const int T = D == 1 ? 512 : (D == 2 ? 32 : 16);
   const int cells = n1 - 1;  // floor bins lie in [0, n1-2]
+  long ncell = cells;
+  if (D >= 2) ncell *= cells;
+  if (D >= 3) ncell *= cells;
+  // cell mode (tile = one cell): the cells fit the tile arrays and hold
+  // enough points each that one block reduction per chunk of a cell is
+  // cheaper than shared-memory atomics that all land on a few nodes
+  const bool cell_mode = ncell <= SGT_HIST_MAX && (long)jp.n >= 64L * ncell;
+  const int T = cell_mode ? 1 : (D == 1 ? 512 : (D == 2 ? 32 : 16));
   const int td = (cells + T - 1) / T;
   int nt = td;
   if (D >= 2) nt *= td;
@@ -168,7 +177,6 @@ k_init_stats(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
   }
 }
 
-#define SGT_HIST_MAX 4096  // tiles held in shared memory by the binning kernels
 
 // ---------------------------------------------------------------------------
 // bin_count: centre (Y = Ynext - mean), zero the grid V, count points per tile
@@ -196,20 +204,30 @@ k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
        g += (long)gridDim.x * blockDim.x)
     V[g] = z;
   __syncthreads();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x) {
-    typename Vec<D>::T y = Ynext[i];
-    int f[3] = {0, 0, 0};
+  // warp-uniform trip count: lanes with the same tile are merged with
+  // match_any and add their count in one shared-memory atomic (points of an
+  // embedding cluster on few tiles)
+  const int lane = threadIdx.x & 31;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i0 = (long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
+    const int i = (int)i0 + lane;
+    int key = -1;
+    if (i < n) {
+      typename Vec<D>::T y = Ynext[i];
+      int f[3] = {0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < D; k++) {
-      const float yc = __fsub_rn(comp<D>(y, k), mean[k]);
-      setcomp<D>(y, k, yc);
-      float sh;
-      const float s = sgt_scale(yc, miny[k], maxy, scale, sh);
-      f[k] = (int)floorf(s);
+      for (int k = 0; k < D; k++) {
+        const float yc = __fsub_rn(comp<D>(y, k), mean[k]);
+        setcomp<D>(y, k, yc);
+        float sh;
+        const float s = sgt_scale(yc, miny[k], maxy, scale, sh);
+        f[k] = (int)floorf(s);
+      }
+      if (write_centred) Y[i] = y;
+      key = sgt_tile_of<D>(f, T, td);
     }
-    if (write_centred) Y[i] = y;
-    atomicAdd(&hist[sgt_tile_of<D>(f, T, td)], 1);
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&hist[key], __popc(grp));
   }
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
@@ -313,33 +331,53 @@ k_bin_scatter(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
   const int lo = blockIdx.x * per, hi = min(n, lo + per);
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x) lc[t] = 0;
   __syncthreads();
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const typename Vec<D>::T y = Y[i];
-    int f[3] = {0, 0, 0};
+  // warp-uniform trip counts; lanes of one tile are merged with match_any,
+  // the group leader does the shared-memory atomic and the lanes take
+  // consecutive slots in lane order
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  for (int i0 = lo + (threadIdx.x & ~31); i0 < hi; i0 += blockDim.x) {
+    const int i = i0 + lane;
+    int key = -1;
+    if (i < hi) {
+      const typename Vec<D>::T y = Y[i];
+      int f[3] = {0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < D; k++) {
-      float sh;
-      f[k] = (int)floorf(sgt_scale(comp<D>(y, k), miny[k], maxy, scale, sh));
+      for (int k = 0; k < D; k++) {
+        float sh;
+        f[k] = (int)floorf(sgt_scale(comp<D>(y, k), miny[k], maxy, scale, sh));
+      }
+      key = sgt_tile_of<D>(f, T, td);
     }
-    atomicAdd(&lc[sgt_tile_of<D>(f, T, td)], 1);
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&lc[key], __popc(grp));
   }
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
     if (lc[t]) lc[t] = atomicAdd(&cursor[t], lc[t]);
   __syncthreads();
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const typename Vec<D>::T y = Y[i];
-    int f[3] = {0, 0, 0};
+  for (int i0 = lo + (threadIdx.x & ~31); i0 < hi; i0 += blockDim.x) {
+    const int i = i0 + lane;
+    int key = -1;
     float4 rec = make_float4(0.f, 0.f, 0.f, __int_as_float(i));
+    if (i < hi) {
+      const typename Vec<D>::T y = Y[i];
+      int f[3] = {0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < D; k++) {
-      float sh;
-      const float v = comp<D>(y, k);
-      f[k] = (int)floorf(sgt_scale(v, miny[k], maxy, scale, sh));
-      if (k == 0) rec.x = v; else if (k == 1) rec.y = v; else rec.z = v;
+      for (int k = 0; k < D; k++) {
+        float sh;
+        const float v = comp<D>(y, k);
+        f[k] = (int)floorf(sgt_scale(v, miny[k], maxy, scale, sh));
+        if (k == 0) rec.x = v; else if (k == 1) rec.y = v; else rec.z = v;
+      }
+      key = sgt_tile_of<D>(f, T, td);
     }
-    const int pos = atomicAdd(&lc[sgt_tile_of<D>(f, T, td)], 1);
-    sorted[pos] = rec;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (key >= 0 && lane == leader) base = atomicAdd(&lc[key], __popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (key >= 0) sorted[base + __popc(grp & below)] = rec;
   }
 }
 
@@ -365,6 +403,7 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
       const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
   extern __shared__ float acc[];  // [D+1][R^D]
   const int T = st->T, td = st->tiles_dim, N = st->N, nch = st->nchunks;
+  if (T == 1) return;  // cell mode: k_s2g_cell does the work
   const float maxy = st->maxy, scale = st->scale;
   // charges are taken about the middle of the grid: F and Z are invariant to
   // the origin of y, and |y - c| <= maxy/2 halves the cancellation in
@@ -447,6 +486,93 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
       }
     }
     __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// S2G in cell mode (T = 1): every point of a chunk lies in the chunk's cell,
+// so all of them touch the same 4^d nodes.  Each thread sums its points'
+// weighted charges in registers (no shared-memory atomics), the block reduces
+// once per chunk, and one global atomic per node and channel goes to V.
+// d = 3 runs in four passes over the z offset of the stencil (64 sums each).
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
+           const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
+  if (st->T != 1) return;  // tile mode: k_s2g does the work
+  constexpr int NN = D == 1 ? 4 : 16;  // stencil nodes per pass
+  constexpr int C = D + 1;             // charge channels
+  constexpr int K = NN * C;
+  constexpr int CS = D == 1 ? 2 : 4;   // floats per node of V
+  constexpr int PASSES = D == 3 ? 4 : 1;
+  __shared__ float red[SGT_THREADS / 32][K];
+  const int td = st->tiles_dim, N = st->N, nch = st->nchunks;
+  const float maxy = st->maxy, scale = st->scale;
+  const float hc = 0.5f * maxy;  // charge origin, as in k_s2g
+  float miny[3];
+#pragma unroll
+  for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  float *Vf = reinterpret_cast<float *>(V);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int4 ch = chunks[c];
+    int cf[3] = {0, 0, 0};
+    cf[0] = ch.x % td;
+    if (D >= 2) cf[1] = (ch.x / td) % td;
+    if (D >= 3) cf[2] = ch.x / (td * td);
+#pragma unroll
+    for (int pass = 0; pass < PASSES; pass++) {
+      float acc[K];
+#pragma unroll
+      for (int q = 0; q < K; q++) acc[q] = 0.f;
+      for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
+        const float4 rec = sorted[j];
+        int f[3];
+        float w[3][4], ys[3];
+        sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
+        bool ok = f[0] == cf[0];
+        if (D >= 2) ok = ok && f[1] == cf[1];
+        if (D >= 3) ok = ok && f[2] == cf[2];
+        if (!ok) {  // the sort and the binning disagree: skip the point
+          atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);
+          continue;
+        }
+        float qc[3];
+#pragma unroll
+        for (int k = 0; k < D; k++) qc[k] = ys[k] - hc;
+        const float wz = D == 3 ? w[2][pass] : 1.f;
+#pragma unroll
+        for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
+          const float wy = (D >= 2 ? w[1][a1] : 1.f) * wz;
+#pragma unroll
+          for (int a0 = 0; a0 < 4; a0++) {
+            const float wt = wy * w[0][a0];
+            const int nd = a1 * 4 + a0;
+            acc[nd * C] += wt;
+#pragma unroll
+            for (int k = 0; k < D; k++) acc[nd * C + 1 + k] += wt * qc[k];
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        const float v = warp_sum_f(acc[q]);
+        if (lane == 0) red[wid][q] = v;
+      }
+      __syncthreads();
+      for (int q = threadIdx.x; q < K; q += blockDim.x) {
+        float sum = 0.f;
+#pragma unroll
+        for (int j = 0; j < SGT_THREADS / 32; j++) sum += red[j][q];
+        const int nd = q / C, chn = q % C;
+        long g = cf[0] + (nd & 3);
+        if (D >= 2) g += (long)N * (cf[1] + (nd >> 2));
+        if (D >= 3) g += (long)N * N * (cf[2] + pass);
+        if (sum != 0.f) atomicAdd(&Vf[g * CS + chn], sum);
+      }
+      __syncthreads();
+    }
   }
 }
 

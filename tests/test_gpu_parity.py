@@ -120,6 +120,45 @@ def test_grids_vs_oracle(torch, ctx, oracle, d):
     assert rel(Phi, Phio) <= 1e-4
 
 
+def cell_mode(n, d, N):
+    """The engine's binning rule: one tile per cell when the (N-3)^d cells fit
+    4096 tiles and hold at least 64 points each on average."""
+    cells = (N - 3) ** d
+    return cells <= 4096 and n >= 64 * cells
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("kind", ["compact", "clusters"])
+def test_cell_mode_vs_oracle(torch, ctx, oracle, d, kind):
+    """Many points on a small grid (the regime of a real run at 1.3M points):
+    the binning keys are cells and S2G sums each cell's points in registers.
+    Charge grid, forces and Z against the oracle at the tolerances above."""
+    import sgtsne_b200 as S
+    n = {1: 20000, 2: 40000, 3: 200000}[d]
+    rng = np.random.default_rng(40 + d)
+    if kind == "compact":
+        Y = (rng.standard_normal((n, d)) * 1.5).astype(np.float32)
+    else:
+        c = rng.standard_normal((6, d)) * 3
+        Y = (c[rng.integers(0, 6, n)] + rng.standard_normal((n, d)) * 0.3).astype(np.float32)
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    Z, N, he = ctx.repulsive(n, d, h, 0, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    assert cell_mode(n, d, N), (n, d, N)
+    V, Phi = ctx.last_grids(d, N)
+    _, sc, sh, N2, mx = oracle.bins_f32(Y, h)
+    assert N2 == N
+    hc = np.float32(0.5) * np.float32(mx)
+    q = np.concatenate([np.ones((n, 1)), (sh - hc).astype(np.float64)], 1)
+    Vo = oracle.s2g(sc.astype(np.float64), q, N)
+    assert rel(V, Vo) <= 1e-5
+    F = f.cpu().numpy().reshape(n, d)
+    Fo, Zo, No, heo = oracle.repulsive_interp(Y.astype(np.float64), h, n1_force=N - 2)
+    assert N == No
+    assert abs(Z - Zo) <= 5e-4 * abs(Zo)
+    assert rel(F, Fo) <= 3e-4
+
+
 @pytest.mark.parametrize("fmt", [0, 2, 3])
 @pytest.mark.parametrize("d", [1, 2, 3])
 def test_attractive_formats(torch, ctx, oracle, fmt, d):
