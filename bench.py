@@ -30,6 +30,11 @@ import time
 
 import numpy as np
 
+# more hardware work queues than the default 8, so the streams of the
+# served jobs (and the branches of a batch graph) do not share queues;
+# read when the CUDA context is created, so set before torch starts CUDA
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "gpu-sg-sne_b200", "python"))
 sys.path.insert(0, REPO)
@@ -214,6 +219,7 @@ def build_problem(args, dev, ctx):
     k = idx.shape[1]
     rp_knn = torch.arange(0, (n + 1) * k, k, dtype=torch.int32, device=dev)
     vals = d2.reshape(-1).contiguous().clone()
+    torch.cuda.synchronize(dev)  # torch's writes complete before the engine reads
     ctx.lambda_bisect(n, rp_knn, vals, 10.0, 1)
     rp_h = rp_knn.cpu().numpy()
     col_h = idx.reshape(-1).cpu().numpy().astype(np.int32)
@@ -323,6 +329,12 @@ def run_ours(args, rank, world, local, dist):
     h2d = (srp.nbytes + sc.nbytes + sv.nbytes + Y0.nbytes) / (W + K)
     d2h = Y0.nbytes / (W + K)
 
+    batched = served = None
+    if rank == 0 and args.batched:
+        batched = run_batched_leg(args, ctx, stream, dev)
+    if rank == 0 and args.served:
+        served = run_served_leg(args, ctx, local)
+
     out = None
     if rank == 0:
         alg = row_alg_bytes(n, nnz, d)
@@ -362,9 +374,79 @@ def run_ours(args, rank, world, local, dist):
                                 f"{W + K} iterations, D2H of Y"},
             "gpu_launches": per_iter_kernels * K,
             "clocks": clk,
+            "batched": batched,
+            "served": served,
         }
     ctx.close()
     return out, (srp, sc, sv, Ystart.cpu().numpy())
+
+
+def run_batched_leg(args, ctx, stream, dev):
+    """The batched configuration (a bounded sample of its 256 instances):
+    plain = each job's iterations one job after another; batched = every
+    job in one CUDA graph.  Embeddings/s = jobs / time of `iters`."""
+    import sgtsne_b200 as S
+    from sgtsne_b200 import multi as Mu
+    t = time.time()
+    inst = Mu.batched_instances(ctx, args.batch_jobs, args.seed, dev)
+    setup = time.time() - t
+    r = Mu.run_batched(S, ctx, inst, args.batch_iters, stream, iters_per_launch=8)
+    njobs = len(inst)
+    out = {"workload": "independent embeddings, n log-uniform in [2000, 200000], dim U{20..100}, "
+                       "isotropic mixture (5-30 components, seed per instance), k=30, lambda=1, "
+                       "half d=2 / half d=3",
+           "jobs": njobs, "of_configured": 256, "iters": args.batch_iters,
+           "total_points": int(sum(i["n"] for i in inst)),
+           "plain_embeds_per_s": njobs / (r["plain_ms"] / 1e3),
+           "batched_embeds_per_s": njobs / (r["batched_ms"] / 1e3),
+           "speedup": r["plain_ms"] / r["batched_ms"], "iters_per_launch": 8,
+           "error_flags": r["error_flags"], "setup_s": round(setup, 1),
+           "timing": "CUDA events on the engine stream; device-resident P and Y0"}
+    return out
+
+
+def run_served_leg(args, ctx, local):
+    """The served configuration (a bounded sample of its 2000 requests):
+    plain = each request alone through the public API, one after another
+    (service times measured, latencies of a FIFO single server under the
+    same arrivals); served = the continuous-batching server under an
+    open-loop Poisson stream at multiples of the plain capacity, and with
+    every request arriving at once (saturation)."""
+    import sgtsne_b200 as S
+    from sgtsne_b200 import multi as Mu
+    t = time.time()
+    req = Mu.request_instances(ctx, args.serve_requests, args.seed + 1, f"cuda:{local}")
+    setup = time.time() - t
+    svc = Mu.plain_service_times(S, ctx, req)
+    cap = 1.0 / float(np.mean(svc))
+    nr = len(req)
+    kw = {"max_active": args.serve_active, "iters_per_round": 16, "rounds_ahead": 2,
+          "hbm_budget": 150 << 30}
+    rows = []
+    for mult in args.serve_rates:
+        rate = mult * cap
+        arr = np.cumsum(np.random.default_rng(args.seed + 3).exponential(1.0 / rate, nr))
+        arr -= arr[0]
+        lat, mk, states = Mu.serve_stream(S, req, arr, device=local, **kw)
+        pl = Mu.fifo_latencies(arr, svc)
+        rows.append({"rate_per_s": rate, "x_plain_capacity": mult,
+                     "served_embeds_per_s": nr / mk,
+                     "served": Mu.percentiles(lat), "plain": Mu.percentiles(pl),
+                     "all_done": all(x == S.REQ_DONE for x in states)})
+    arr = np.zeros(nr)
+    lat, mk, states = Mu.serve_stream(S, req, arr, device=local, **kw)
+    pl = Mu.fifo_latencies(arr, svc)
+    sat = {"served_embeds_per_s": nr / mk, "plain_embeds_per_s": cap,
+           "speedup": (nr / mk) / cap, "served": Mu.percentiles(lat),
+           "plain": Mu.percentiles(pl), "all_done": all(x == S.REQ_DONE for x in states)}
+    return {"workload": "requests with n log-uniform in [1000, 500000], d in {2,3}, "
+                        "lambda in {1,10,30}, 500-1000 iterations, P from the 50-D 40-component "
+                        "Zipf(1.1) mixture (seed per request), 150 GB HBM budget",
+            "requests": nr, "of_configured": 2000,
+            "total_points": int(sum(i["n"] for i in req)),
+            "plain_service_s": {"mean": float(np.mean(svc)), "sum": float(np.sum(svc))},
+            "server": kw, "open_loop": rows, "saturation": sat, "setup_s": round(setup, 1),
+            "latency": "scheduled arrival to coordinates in the caller's host buffer"}
 
 
 def cpu_sample(srp, sc, sv, Ystate, iters, threads):
@@ -430,6 +512,15 @@ def main():
     ap.add_argument("--no-expanded", dest="expanded", action="store_false",
                     help="skip the fixed expanded-state (largest grid) line")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="skip the batched-embeddings line")
+    ap.add_argument("--batch-jobs", type=int, default=64)
+    ap.add_argument("--batch-iters", type=int, default=1000)
+    ap.add_argument("--no-served", dest="served", action="store_false",
+                    help="skip the served request-stream line")
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-active", type=int, default=32)
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[2.0, 4.0])
     args = ap.parse_args()
     rank, world, local = dist_env()
     import torch

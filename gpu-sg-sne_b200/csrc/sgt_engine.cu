@@ -72,7 +72,8 @@ struct sgt_job {
   SgtState *st_host = nullptr;
   int nb_pts = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0, nb_part = 0;
   size_t smem_s2g = 0, smem_fft1 = 0, smem_fft2 = 0;
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr;        // one iteration
+  cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
   double last_kl = 0.0;
   float tune_ms[4] = {0, 0, 0, 0};  // row kernel ms for G = 4, 8, 16, 32
@@ -116,6 +117,16 @@ static sgt_status jalloc(sgt_job *J, T **ptr, size_t count) {
 }
 
 static int grid_blocks(int nsm, int per_sm) { return std::max(1, nsm * std::max(1, per_sm)); }
+
+// iterations per launch of a job's chained graph (sgt_job_run)
+#define SGT_GRAPH_ITERS 16
+
+static void drop_graphs(sgt_job *J) {
+  if (J->gexec) cudaGraphExecDestroy(J->gexec);
+  if (J->gexec_multi) cudaGraphExecDestroy(J->gexec_multi);
+  J->gexec = nullptr;
+  J->gexec_multi = nullptr;
+}
 
 extern "C" {
 
@@ -744,10 +755,7 @@ static sgt_status relayout_d(sgt_job *J) {
     J->perm_alt = nullptr;
     CKS(jalloc(J, &J->perm_alt, (size_t)n));
   }
-  if (J->gexec) {  // buffers moved: capture the iteration again
-    cudaGraphExecDestroy(J->gexec);
-    J->gexec = nullptr;
-  }
+  drop_graphs(J);  // buffers moved: capture the iteration again
   J->relayouts++;
   return SGT_OK;
 }
@@ -922,7 +930,7 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
 void sgt_job_destroy(sgt_job *J) {
   if (!J) return;
   if (J->ctx) cudaSetDevice(J->ctx->device);
-  if (J->gexec) cudaGraphExecDestroy(J->gexec);
+  drop_graphs(J);
   if (J->ctx) {
     cudaStream_t s = J->ctx->stream;
     for (void *p : J->allocs) cudaFreeAsync(p, s);
@@ -970,13 +978,60 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
   return SGT_OK;
 }
 
-static sgt_status run_one(sgt_job *J);
+// Capture `iters` chained iterations of a job into a graph (the kernels read
+// every per-iteration size from the device-side state, so one capture
+// serves every iteration).
+static sgt_status capture_graph(sgt_job *J, int iters, cudaGraph_t *out) {
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  *out = nullptr;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  sgt_status es = SGT_OK;
+  for (int r = 0; r < iters && es == SGT_OK; r++) es = dispatch_iteration(J, s);
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (es != SGT_OK) {
+    if (g) cudaGraphDestroy(g);
+    return es;
+  }
+  CK(ce);
+  *out = g;
+  return SGT_OK;
+}
+
+static sgt_status instantiate(sgt_job *J, int iters, cudaGraphExec_t *exec) {
+  sgt_ctx *ctx = J->ctx;
+  cudaGraph_t g = nullptr;
+  CKS(capture_graph(J, iters, &g));
+  cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  CK(ie);
+  return SGT_OK;
+}
+
+static sgt_status run_one(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
+  if (!J->gexec) CKS(instantiate(J, 1, &J->gexec));
+  CK(cudaGraphLaunch(J->gexec, ctx->stream));
+  return SGT_OK;
+}
+
 sgt_status sgt_job_run(sgt_job *J, int iters) {
   if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
   sgt_ctx *ctx = J->ctx;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
   const int every = J->p.relayout_every;
+  if (every <= 0 && J->p.kl_every <= 0) {
+    // nothing happens between iterations: chained graphs of 16 iterations
+    int left = iters;
+    if (left >= SGT_GRAPH_ITERS && !J->gexec_multi)
+      CKS(instantiate(J, SGT_GRAPH_ITERS, &J->gexec_multi));
+    for (; left >= SGT_GRAPH_ITERS; left -= SGT_GRAPH_ITERS) CK(cudaGraphLaunch(J->gexec_multi, s));
+    for (; left > 0; left--) CKS(run_one(J));
+    J->host_iter += iters;
+    return SGT_OK;
+  }
   for (int it = 0; it < iters; it++) {
     if (every > 0 && J->host_iter > 0 && J->host_iter % every == 0) CKS(relayout(J));
     CKS(run_one(J));
@@ -990,25 +1045,127 @@ sgt_status sgt_job_run(sgt_job *J, int iters) {
   return SGT_OK;
 }
 
-static sgt_status run_one(sgt_job *J) {
-  sgt_ctx *ctx = J->ctx;
-  cudaStream_t s = ctx->stream;
-  if (!J->gexec) {
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    sgt_status es = dispatch_iteration(J, s);
-    cudaError_t ce = cudaStreamEndCapture(s, &g);
-    if (es != SGT_OK) {
-      if (g) cudaGraphDestroy(g);
-      return es;
+// ---------------------------------------------------------------------------
+// batches: one graph, one branch of R chained iterations per job
+// ---------------------------------------------------------------------------
+struct sgt_batch {
+  sgt_ctx *ctx = nullptr;
+  std::vector<sgt_job *> jobs;
+  int R = 1;
+  cudaGraphExec_t exec_r = nullptr, exec_1 = nullptr;
+};
+
+static sgt_status batch_build(sgt_batch *b, const std::vector<cudaGraph_t> &iter_graphs, int R,
+                              cudaGraphExec_t *exec) {
+  sgt_ctx *ctx = b->ctx;
+  cudaGraph_t parent = nullptr;
+  CK(cudaGraphCreate(&parent, 0));
+  for (cudaGraph_t g : iter_graphs) {
+    cudaGraphNode_t prev = nullptr;
+    for (int r = 0; r < R; r++) {
+      cudaGraphNode_t node = nullptr;
+      const cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, prev ? &prev : nullptr,
+                                                       prev ? 1 : 0, g);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(parent);
+        return fail(ctx, SGT_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+      }
+      prev = node;
     }
-    CK(ce);
-    cudaError_t ie = cudaGraphInstantiate(&J->gexec, g, 0);
-    cudaGraphDestroy(g);
-    CK(ie);
   }
-  CK(cudaGraphLaunch(J->gexec, s));
+  const cudaError_t ie = cudaGraphInstantiate(exec, parent, 0);
+  cudaGraphDestroy(parent);
+  CK(ie);
   return SGT_OK;
+}
+
+sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int iters_per_launch,
+                            sgt_batch **out) {
+  if (!ctx || !out || njobs < 1 || !jobs || iters_per_launch < 1 || iters_per_launch > 256)
+    return SGT_ERR_INVALID_ARG;
+  *out = nullptr;
+  for (int k = 0; k < njobs; k++) {
+    if (!jobs[k] || jobs[k]->ctx != ctx)
+      return fail(ctx, SGT_ERR_INVALID_ARG, "batch jobs must belong to the batch's context");
+    if (jobs[k]->p.relayout_every > 0 || jobs[k]->p.kl_every > 0)
+      return fail(ctx, SGT_ERR_UNSUPPORTED, "batch jobs cannot relayout or record KL in the loop");
+  }
+  CK(cudaSetDevice(ctx->device));
+  sgt_batch *b = new sgt_batch();
+  b->ctx = ctx;
+  b->jobs.assign(jobs, jobs + njobs);
+  b->R = iters_per_launch;
+  std::vector<cudaGraph_t> gs;
+  sgt_status st = SGT_OK;
+  for (int k = 0; k < njobs && st == SGT_OK; k++) {
+    cudaGraph_t g = nullptr;
+    st = capture_graph(jobs[k], 1, &g);
+    if (st == SGT_OK) gs.push_back(g);
+  }
+  if (st == SGT_OK) st = batch_build(b, gs, b->R, &b->exec_r);
+  if (st == SGT_OK && b->R > 1) st = batch_build(b, gs, 1, &b->exec_1);
+  for (cudaGraph_t g : gs) cudaGraphDestroy(g);
+  if (st != SGT_OK) {
+    sgt_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return SGT_OK;
+}
+
+sgt_status sgt_batch_run(sgt_batch *b, int iters) {
+  if (!b || iters < 0) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = b->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  int left = iters;
+  for (; left >= b->R; left -= b->R) CK(cudaGraphLaunch(b->exec_r, s));
+  for (; left > 0; left--) CK(cudaGraphLaunch(b->R > 1 ? b->exec_1 : b->exec_r, s));
+  for (sgt_job *J : b->jobs) J->host_iter += iters;
+  return SGT_OK;
+}
+
+void sgt_batch_destroy(sgt_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx->device);
+  if (b->exec_r) cudaGraphExecDestroy(b->exec_r);
+  if (b->exec_1) cudaGraphExecDestroy(b->exec_1);
+  delete b;
+}
+
+// Device bytes of a job: the buffers of job_alloc, job_alloc_parts and P,
+// plus the largest transient of job creation (host P staged on the device,
+// or the autotuner's scratch copies).
+size_t sgt_job_footprint(const sgt_params *p, int n, long nnz) {
+  if (!p || n < 1 || nnz < 0 || p->d < 1 || p->d > 3) return 0;
+  const int D = p->d, S = D == 3 ? 4 : D;
+  const size_t np = (size_t)n * S;
+  size_t b = 5 * np * 4 + (size_t)n * 16;  // Y, Ynext, uY, gains, Frep; sorted
+  int max_grid = p->max_grid > 0 ? p->max_grid : (D <= 2 ? 512 : 128);
+  max_grid = std::min(D == 3 ? 256 : 512, std::max(16, max_grid));
+  size_t M = 1;
+  while (M < (size_t)(2 * max_grid - 1)) M <<= 1;
+  if (D == 1) M = std::max<size_t>(M, 32);
+  size_t nmax = std::min<size_t>(512, (M + 1) / 2), nodes = nmax, plane = M;
+  if (D >= 2) { nodes *= nmax; plane *= M; }
+  if (D >= 3) { nodes *= nmax; plane *= M; }
+  b += 2 * nodes * (D == 1 ? 2 : 4) * 4;                       // V, Phi
+  if (D >= 2) b += 3 * plane * 8;                               // FFT planes
+  b += 2 * 4096 * 4 + ((size_t)n / 1024 + 4096 + 16) * 16;       // tiles, chunks
+  const size_t parts = std::max<size_t>(148 * 16, ((size_t)n * 32 + 255) / 256);
+  b += parts * (16 + 16 + 32 + 8 + 8) + 1024;                   // partials, state
+  b += ((size_t)n + 1) * 4;                                     // rowptr
+  size_t transient = 8 * (size_t)nnz;                           // staged col/val
+  if (p->format == SGT_FORMAT_CSR) {
+    b += ((size_t)nnz + 8) * 8;
+    transient = std::max(transient, 4 * np * 4);
+  } else if (p->format == SGT_FORMAT_COO) {
+    b += 12 * (size_t)nnz + np * 4;  // rows, cols, vals; Fattr
+  } else {
+    // ELL of width W (the CUSP rule keeps n*W below 3 nnz) and the COO tail
+    b += 36 * (size_t)nnz + np * 4;
+  }
+  return b + transient;
 }
 
 sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, int centre) {

@@ -4,6 +4,12 @@ The engine is CUDA + C++ behind a C ABI; this module only marshals
 arguments.  Device buffers are passed as torch CUDA tensors (used purely as
 device memory), host buffers as numpy arrays.  There is no fallback: if the
 shared library is missing, load() raises.
+
+Ordering: the engine queues its work on the context's stream (its own
+non-blocking stream unless Context.set_stream names another).  Tensors that
+torch writes on a different stream must be complete (synchronise, or share
+the stream with set_stream) before an engine call reads them, and engine
+results must be complete before torch reads them.
 """
 from __future__ import annotations
 
@@ -48,6 +54,19 @@ class JobInfo(C.Structure):
                 ("nnz", C.c_long), ("row_group", C.c_int), ("tune_ms", C.c_float * 4)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_active", C.c_int),
+                ("iters_per_round", C.c_int), ("rounds_ahead", C.c_int)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("n", C.c_int), ("d", C.c_int),
+                ("iters", C.c_int), ("footprint", C.c_size_t), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+REQ_WAITING, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
 # every symbol the header declares, with (restype, argtypes)
 _vp, _i, _l, _f, _d = C.c_void_p, C.c_int, C.c_long, C.c_float, C.c_double
 SIGNATURES = {
@@ -67,6 +86,18 @@ SIGNATURES = {
     "sgt_job_get_info": (_i, [_vp, C.POINTER(JobInfo)]),
     "sgt_job_kl": (_i, [_vp, _d, C.POINTER(_d)]),
     "sgt_job_profile": (_i, [_vp, _i, _vp]),
+    "sgt_batch_create": (_i, [_vp, _i, C.POINTER(_vp), _i, C.POINTER(_vp)]),
+    "sgt_batch_run": (_i, [_vp, _i]),
+    "sgt_batch_destroy": (None, [_vp]),
+    "sgt_job_footprint": (C.c_size_t, [C.POINTER(Params), _i, _l]),
+    "sgt_server_config_default": (None, [C.POINTER(ServerConfig)]),
+    "sgt_server_create": (_i, [_i, C.POINTER(ServerConfig), C.POINTER(_vp)]),
+    "sgt_server_destroy": (None, [_vp]),
+    "sgt_server_submit": (_i, [_vp, C.POINTER(Params), _i, _vp, _vp, _vp, _vp, _vp,
+                               C.POINTER(C.c_longlong)]),
+    "sgt_server_poll": (_i, [_vp, _d, C.POINTER(C.c_longlong), _i, C.POINTER(_i)]),
+    "sgt_server_request_info": (_i, [_vp, C.c_longlong, C.POINTER(RequestInfo)]),
+    "sgt_server_now": (_d, [_vp]),
     "sgt_attractive": (_i, [_vp, _i, _i, _i, _l, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "sgt_repulsive": (_i, [_vp, _i, _i, _f, _i, _vp, _i, _vp, C.POINTER(_d),
                            C.POINTER(_i), C.POINTER(_f)]),
@@ -271,6 +302,114 @@ class Job:
         ms = np.zeros(8, np.float64)
         self.ctx.check(self.lib.sgt_job_profile(self.h, int(iters), _ptr(ms)), "profile")
         return ms
+
+
+class Batch:
+    """Jobs of one context advanced together through one CUDA graph
+    (sgt_batch_*).  The jobs must stay open while the batch is used."""
+
+    def __init__(self, ctx: Context, jobs, iters_per_launch=8):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.jobs = list(jobs)
+        arr = (C.c_void_p * len(self.jobs))(*[j.h for j in self.jobs])
+        h = C.c_void_p()
+        ctx.check(self.lib.sgt_batch_create(ctx.h, len(self.jobs), arr, int(iters_per_launch),
+                                            C.byref(h)), "batch_create")
+        self.h = h
+
+    def run(self, iters):
+        self.ctx.check(self.lib.sgt_batch_run(self.h, int(iters)), "batch_run")
+
+    def close(self):
+        if self.h:
+            self.lib.sgt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def job_footprint(params: Params, n: int, nnz: int) -> int:
+    return int(load().sgt_job_footprint(C.byref(params), int(n), int(nnz)))
+
+
+class Server:
+    """Continuous-batching request server (sgt_server_*).  Host numpy
+    buffers of a request are kept referenced here until it finishes."""
+
+    def __init__(self, device=0, hbm_budget=None, max_active=None, iters_per_round=None,
+                 rounds_ahead=None):
+        self.lib = load()
+        cfg = ServerConfig()
+        self.lib.sgt_server_config_default(C.byref(cfg))
+        if hbm_budget is not None:
+            cfg.hbm_budget = int(hbm_budget)
+        if max_active is not None:
+            cfg.max_active = int(max_active)
+        if iters_per_round is not None:
+            cfg.iters_per_round = int(iters_per_round)
+        if rounds_ahead is not None:
+            cfg.rounds_ahead = int(rounds_ahead)
+        self.cfg = cfg
+        h = C.c_void_p()
+        st = self.lib.sgt_server_create(int(device), C.byref(cfg), C.byref(h))
+        if st != 0:
+            raise SgtError(st, "server_create")
+        self.h = h
+        self._keep = {}
+
+    def submit(self, params: Params, rowptr, col, val, y0):
+        """Returns (request id, output array filled when the request is done)."""
+        rowptr = np.ascontiguousarray(rowptr, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        val = np.ascontiguousarray(val, np.float32)
+        y0 = np.ascontiguousarray(y0, np.float32)
+        n = len(rowptr) - 1
+        out = np.empty((n, params.d), np.float32)
+        rid = C.c_longlong()
+        st = self.lib.sgt_server_submit(self.h, C.byref(params), n, _ptr(rowptr), _ptr(col),
+                                        _ptr(val), _ptr(y0), _ptr(out), C.byref(rid))
+        if st != 0:
+            raise SgtError(st, "server_submit")
+        self._keep[rid.value] = (rowptr, col, val, y0, out)
+        return rid.value, out
+
+    def poll(self, wait_ms=0.0, cap=256):
+        ids = (C.c_longlong * cap)()
+        cnt = C.c_int()
+        st = self.lib.sgt_server_poll(self.h, float(wait_ms), ids, cap, C.byref(cnt))
+        if st != 0:
+            raise SgtError(st, "server_poll")
+        done = [ids[k] for k in range(cnt.value)]
+        for r in done:
+            self._keep.pop(r, None)
+        return done
+
+    def info(self, rid) -> RequestInfo:
+        inf = RequestInfo()
+        st = self.lib.sgt_server_request_info(self.h, int(rid), C.byref(inf))
+        if st != 0:
+            raise SgtError(st, "server_request_info")
+        return inf
+
+    def now(self):
+        return self.lib.sgt_server_now(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.sgt_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---- host-side helpers (no device) ----

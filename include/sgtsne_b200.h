@@ -152,6 +152,82 @@ sgt_status sgt_job_kl(sgt_job *job, double alpha, double *kl);
    stage_ms[8] = {bin, s2g, g2g, g2s, attractive+update, total, -, -}. */
 sgt_status sgt_job_profile(sgt_job *job, int iters, double *stage_ms);
 
+/* ---- batches: many independent embeddings advanced together -----------
+ * No counterpart in the reference, which runs one embedding per process
+ * (CU/sgtsne.cu:25-129).  A batch holds jobs of one context.  sgt_batch_run
+ * advances every job by the same number of iterations through one CUDA graph
+ * whose independent branches are the jobs' iterations (iters_per_launch
+ * chained iterations per branch), so the kernels of small embeddings run
+ * side by side instead of one job after another.  Jobs keep their own state
+ * (sgt_job_get_y, sgt_job_get_info work as usual) and must outlive the batch.
+ * Jobs with relayout_every or kl_every set return SGT_ERR_UNSUPPORTED. */
+typedef struct sgt_batch sgt_batch;
+sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs,
+                            int iters_per_launch, sgt_batch **out);
+/* Queue `iters` iterations of every job; asynchronous like sgt_job_run. */
+sgt_status sgt_batch_run(sgt_batch *batch, int iters);
+void sgt_batch_destroy(sgt_batch *batch);
+
+/* Device bytes a job of these dimensions holds at its peak (creation
+   included); what the server admits against its budget. */
+size_t sgt_job_footprint(const sgt_params *params, int n, long nnz);
+
+/* ---- serving: continuous batching of embedding requests ---------------
+ * No counterpart in the reference.  A server on one device holds an HBM
+ * budget and up to max_active running jobs, each on its own stream (stream
+ * priority rises as n falls, so short requests are not stuck behind long
+ * ones).  An admission thread turns waiting requests into jobs, in FIFO
+ * order, as soon as their footprint fits the budget and a slot is free; a
+ * scheduler thread keeps every running job `rounds_ahead` rounds of
+ * `iters_per_round` iterations ahead of the GPU (one graph launch per
+ * round), copies a finished job's coordinates to the caller's buffer and
+ * returns its memory to the budget.  Requests that arrive while others run
+ * are admitted while those are still on the GPU; their kernels overlap. */
+typedef struct sgt_server sgt_server;
+typedef struct {
+  size_t hbm_budget;   /* device bytes the running jobs may hold          */
+  int max_active;      /* running jobs (streams), 1..1024                 */
+  int iters_per_round; /* iterations per graph launch, 1..256             */
+  int rounds_ahead;    /* rounds queued ahead of the GPU per job, >= 1    */
+} sgt_server_config;
+typedef enum {
+  SGT_REQ_WAITING = 0,
+  SGT_REQ_RUNNING = 1,
+  SGT_REQ_DONE = 2,
+  SGT_REQ_FAILED = 3
+} sgt_request_state;
+typedef struct {
+  int state;           /* sgt_request_state                               */
+  sgt_status status;   /* why a request failed                            */
+  int n, d, iters;     /* request dimensions                              */
+  size_t footprint;    /* bytes admitted against the budget               */
+  double t_submit;     /* seconds since the server was created (steady    */
+  double t_admit;      /*   clock): submission, admission and the moment  */
+  double t_done;       /*   its coordinates were in the caller's buffer   */
+} sgt_request_info;
+void sgt_server_config_default(sgt_server_config *cfg);
+sgt_status sgt_server_create(int device, const sgt_server_config *cfg,
+                             sgt_server **out);
+/* Waits for running jobs to finish, then frees everything. */
+void sgt_server_destroy(sgt_server *srv);
+/* Queue a request.  rowptr/col/val: host CSR of the symmetric, normalised P
+   (as sgt_job_create); y0 and y_out: host, point-major n*d.  All caller-owned
+   and kept alive until the request is done or failed.  params->max_iter is
+   the number of iterations; the result is centred as after the reference's
+   last iteration.  *id receives the request id (0, 1, 2, ...). */
+sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n,
+                             const int *rowptr, const int *col,
+                             const float *val, const float *y0, float *y_out,
+                             long long *id);
+/* Ids of requests finished (done or failed) since the last call, up to cap;
+   waits up to wait_ms for at least one when none is ready. */
+sgt_status sgt_server_poll(sgt_server *srv, double wait_ms, long long *ids,
+                           int cap, int *count);
+sgt_status sgt_server_request_info(sgt_server *srv, long long id,
+                                   sgt_request_info *info);
+/* Seconds on the server's clock (the time base of sgt_request_info). */
+double sgt_server_now(const sgt_server *srv);
+
 /* ---- stage operators (device pointers, queued on the context stream) --- */
 
 /* F_attr = sum_j p_ij (y_i - y_j)/(1+|y_i-y_j|^2).  Replaces

@@ -81,3 +81,18 @@ def test_symmetrize_rejects_bad_columns(S):
     col = np.array([1, 5], np.int32)
     with pytest.raises(S.SgtError):
         S.symmetrize(rp, col, np.ones(2, np.float32), 1.0)
+
+
+def test_job_footprint_host_rule(S):
+    """Admission footprint: host arithmetic only (no device), monotone in n
+    and nnz, larger for d = 3 (FFT planes of M^3), zero for bad input."""
+    p2 = S.default_params(d=2, format=S.FORMAT_CSR)
+    p3 = S.default_params(d=3, format=S.FORMAT_CSR)
+    a = S.job_footprint(p2, 10000, 300000)
+    assert a > 8 * 300000
+    assert S.job_footprint(p2, 20000, 300000) > a
+    assert S.job_footprint(p2, 10000, 600000) > a
+    assert S.job_footprint(p3, 10000, 300000) > a
+    assert S.job_footprint(S.default_params(d=4), 10000, 10) == 0
+    small = S.default_params(d=3, format=S.FORMAT_CSR, max_grid=64)
+    assert S.job_footprint(small, 10000, 300000) < S.job_footprint(p3, 10000, 300000)
