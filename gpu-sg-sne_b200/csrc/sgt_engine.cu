@@ -28,6 +28,10 @@ struct sgt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // branch stream of an iteration: the attractive SpMV runs on it beside the
+  // repulsion chain on `stream` (forked and joined with events, so captured
+  // graphs get two parallel branches)
+  cudaStream_t side = nullptr;
   int nsm = 148;
   std::string err;
   sgt_job *scratch = nullptr;  // buffers of the operator entry points
@@ -70,7 +74,9 @@ struct sgt_job {
   double *part_sum = nullptr, *part_z = nullptr, *part_kl = nullptr;
   SgtState *st = nullptr;
   SgtState *st_host = nullptr;
-  int nb_pts = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0, nb_part = 0;
+  int nb_pts = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0,
+      nb_upd = 0, nb_part = 0;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // the two branches of an iteration
   size_t smem_s2g = 0, smem_fft1 = 0, smem_fft2 = 0;
   cudaGraphExec_t gexec = nullptr;        // one iteration
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
@@ -194,7 +200,9 @@ sgt_status sgt_create(int device, sgt_ctx **out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SGT_ERR_CUDA;
   }
@@ -210,6 +218,7 @@ void sgt_destroy(sgt_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->scratch) sgt_job_destroy(ctx->scratch);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
   delete ctx;
 }
 
@@ -304,6 +313,8 @@ static sgt_status job_shapes(sgt_job *J) {
     default: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 32, true>, SGT_THREADS, 0)); break;
   }
   J->nb_row = grid_blocks(nsm, occ);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 1, false>, SGT_THREADS, 0));
+  J->nb_upd = grid_blocks(nsm, occ);
   // small embeddings launch no more blocks than there is work for: idle
   // blocks only take scheduling slots from the jobs that share the GPU
   const int cap = (int)std::max(1L, ((long)J->n + 255) / 256);
@@ -312,14 +323,14 @@ static sgt_status job_shapes(sgt_job *J) {
   J->nb_s2gc = std::min(J->nb_s2gc, cap);
   J->nb_g2s = std::min(J->nb_g2s, cap);
   J->nb_row = std::min(J->nb_row, cap);
+  J->nb_upd = std::min(J->nb_upd, cap);
   if constexpr (D == 2) {  // lines of the largest grid this job can take
     const int lines_rows = 2 * J->nmax + J->mmax, lines_cols = J->mmax / SGT_FFT_COLS;
     J->nb_fft_rows = std::min(J->nb_fft_rows, (lines_rows + 7) / 8);
     J->nb_fft = std::min(J->nb_fft, std::max(1, lines_cols));
   }
   J->nb_part = std::max(std::max(J->nb_pts, J->nb_row), std::max(J->nb_g2s, J->nb_s2g));
-  // the fused CSR row kernel launches ceil(n * G / 256) blocks, G <= 32
-  J->nb_part = std::max(J->nb_part, (int)(((long)J->n * 32 + SGT_THREADS - 1) / SGT_THREADS));
+  J->nb_part = std::max(J->nb_part, J->nb_upd);
   return SGT_OK;
 }
 
@@ -361,6 +372,8 @@ static sgt_status job_alloc(sgt_job *J) {
   J->jp.tile_cap = SGT_HIST_MAX;
   CKS(jalloc(J, &J->st, 1));
   J->st_host = new SgtState();
+  CK(cudaEventCreateWithFlags(&J->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&J->ev_join, cudaEventDisableTiming));
   CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, ctx->stream));
   CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), ctx->stream));
   return SGT_OK;
@@ -436,15 +449,26 @@ static sgt_status enqueue_g2g(sgt_job *J, cudaStream_t s) {
   return SGT_OK;
 }
 
-// ev (optional): events recorded after the binning, S2G and G2G stages
+// Centre Ynext into Y, count points per tile, zero the charge grid.
 template <int D>
-static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+static sgt_status enqueue_bin_count(sgt_job *J, cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  typedef typename Vec<D>::T VT;
+  typedef typename Node<D>::T NT;
+  k_bin_count<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n,
+                                                   J->st, J->tile_count, (NT *)J->V, 1);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+// The rest of the repulsion: tile offsets, sort, S2G, G2G, G2S and Z.
+// ev (optional): events recorded after the binning, S2G and G2G stages.
+template <int D>
+static sgt_status enqueue_repulsion_rest(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   typedef typename Node<D>::T NT;
   const int n = J->n;
-  k_bin_count<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, n,
-                                                   J->st, J->tile_count, (NT *)J->V, 1);
   k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
   k_bin_scatter<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, n, J->st, J->cursor,
                                                      J->sorted);
@@ -461,18 +485,22 @@ static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s, cudaEvent_t *ev 
   return SGT_OK;
 }
 
+template <int D>
+static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+  CKS(enqueue_bin_count<D>(J, s));
+  return enqueue_repulsion_rest<D>(J, s, ev);
+}
+
+// F_attr of the centred Y in the job's format
 template <int D, int G>
-static sgt_status enqueue_update(sgt_job *J, cudaStream_t s) {
+static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   const int n = J->n;
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    k_row_fused<D, G><<<nb, SGT_THREADS, 0, s>>>(
-        J->rowptr, J->pairs, (const VT *)J->Y, (const VT *)J->Frep, (VT *)J->uY, (VT *)J->gains,
-        (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max, J->part_sum);
-    k_iter_stats<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, J->st, J->jp,
-                                                      J->part_min, J->part_max, J->part_sum);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)J->Y,
+                                                 (VT *)J->Fattr, n);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals,
@@ -483,24 +511,51 @@ static sgt_status enqueue_update(sgt_job *J, cudaStream_t s) {
     if (J->coo_n > 0)
       k_attr_coo<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(J->coo_n, J->coo_rows, J->coo_cols,
                                                       J->coo_vals, (const VT *)J->Y, J->Fattr);
-    k_row_update<D, G, false><<<J->nb_row, SGT_THREADS, 0, s>>>(
-        nullptr, nullptr, (const VT *)J->Fattr, (const VT *)J->Y, (const VT *)J->Frep,
-        (VT *)J->uY, (VT *)J->gains, (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max,
-        J->part_sum);
   }
   CK(cudaGetLastError());
   return SGT_OK;
 }
 
 template <int D>
-static sgt_status enqueue_iteration(sgt_job *J, cudaStream_t s) {
-  CKS(enqueue_repulsion<D>(J, s));
+static sgt_status dispatch_attractive(sgt_job *J, cudaStream_t s) {
   switch (J->G) {
-    case 4: return enqueue_update<D, 4>(J, s);
-    case 8: return enqueue_update<D, 8>(J, s);
-    case 16: return enqueue_update<D, 16>(J, s);
-    default: return enqueue_update<D, 32>(J, s);
+    case 4: return enqueue_attractive<D, 4>(J, s);
+    case 8: return enqueue_attractive<D, 8>(J, s);
+    case 16: return enqueue_attractive<D, 16>(J, s);
+    default: return enqueue_attractive<D, 32>(J, s);
   }
+}
+
+// dY, gains, momentum, Ynext, and the min/max/sum of Ynext that decide the
+// next iteration's grid (one point per thread)
+template <int D>
+static sgt_status enqueue_combine(sgt_job *J, cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  typedef typename Vec<D>::T VT;
+  k_row_update<D, 1, false><<<J->nb_upd, SGT_THREADS, 0, s>>>(
+      nullptr, nullptr, (const VT *)J->Fattr, (const VT *)J->Y, (const VT *)J->Frep,
+      (VT *)J->uY, (VT *)J->gains, (VT *)J->Ynext, J->st, J->jp, J->part_min, J->part_max,
+      J->part_sum);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+// One iteration.  After the binning pass has written the centred Y, the
+// attractive SpMV (bound by L1 gather throughput) and the rest of the
+// repulsion chain (a series of latency-bound kernels) both read only Y:
+// the SpMV is forked onto the context's side stream and joined before the
+// combine, so in the captured graph the two run concurrently.
+template <int D>
+static sgt_status enqueue_iteration(sgt_job *J, cudaStream_t s) {
+  sgt_ctx *ctx = J->ctx;
+  CKS(enqueue_bin_count<D>(J, s));
+  CK(cudaEventRecord(J->ev_fork, s));
+  CK(cudaStreamWaitEvent(ctx->side, J->ev_fork, 0));
+  CKS(dispatch_attractive<D>(J, ctx->side));
+  CK(cudaEventRecord(J->ev_join, ctx->side));
+  CKS(enqueue_repulsion_rest<D>(J, s));
+  CK(cudaStreamWaitEvent(s, J->ev_join, 0));
+  return enqueue_combine<D>(J, s);
 }
 
 static sgt_status dispatch_iteration(sgt_job *J, cudaStream_t s) {
@@ -616,22 +671,20 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
 
 
 // ---------------------------------------------------------------------------
-// autotuner: lanes per row of the fused row kernel, timed on this job's P
-// (scratch copies of every array the kernel writes; the job's state is not
-// touched).  The fastest of G = 4, 8, 16, 32 is kept.
+// autotuner: lanes per row of the attractive SpMV, timed on this job's P
+// (scratch input and output arrays; the job's state is not touched).  The
+// fastest of G = 4, 8, 16, 32 is kept.
 // ---------------------------------------------------------------------------
 template <int D, int G>
-static float time_row_kernel(sgt_job *J, float *tY, float *tU, float *tG, float *tYn,
-                             SgtState *tst, cudaEvent_t e0, cudaEvent_t e1) {
+static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1) {
   typedef typename Vec<D>::T VT;
   cudaStream_t s = J->ctx->stream;
   float best = 1e30f;
-  for (int rep = 0; rep < 4; rep++) {
+  for (int rep = 0; rep < 4; rep++) {  // the first launch warms caches
     cudaEventRecord(e0, s);
     const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-    k_row_fused<D, G><<<nb, SGT_THREADS, 0, s>>>(
-        J->rowptr, J->pairs, (const VT *)tY, (const VT *)J->Frep, (VT *)tU, (VT *)tG, (VT *)tYn,
-        tst, J->jp, J->part_min, J->part_max, J->part_sum);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY, (VT *)tF,
+                                                 J->n);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -647,31 +700,23 @@ static sgt_status tune_group_d(sgt_job *J) {
   cudaStream_t s = ctx->stream;
   const size_t np = (size_t)J->n * J->S;
   float *buf = nullptr;
-  SgtState *tst = nullptr;
-  CK(cudaMallocAsync(&buf, sizeof(float) * np * 4, s));
-  CK(cudaMallocAsync(&tst, sizeof(SgtState), s));
-  CK(cudaMemsetAsync(buf, 0, sizeof(float) * np * 4, s));
-  CK(cudaMemsetAsync(J->Frep, 0, sizeof(float) * np, s));
-  SgtState h;
-  memset(&h, 0, sizeof(h));
-  h.Z = 1.0;
-  h.N = 16; h.M = 32; h.logM = 5; h.maxy = 1.f; h.scale = 13.f; h.T = 32; h.tiles_dim = 1; h.ntiles = 1;
-  CK(cudaMemcpyAsync(tst, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  CK(cudaMallocAsync(&buf, sizeof(float) * np * 2, s));
+  CK(cudaMemsetAsync(buf, 0, sizeof(float) * np * 2, s));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  float *tY = buf, *tU = buf + np, *tG = buf + 2 * np, *tYn = buf + 3 * np;
+  const float *tY = buf;  // zero coordinates: the gather pattern of P, finite values
+  float *tF = buf + np;
   const int cand[4] = {4, 8, 16, 32};
   float t[4];
-  t[0] = time_row_kernel<D, 4>(J, tY, tU, tG, tYn, tst, e0, e1);
-  t[1] = time_row_kernel<D, 8>(J, tY, tU, tG, tYn, tst, e0, e1);
-  t[2] = time_row_kernel<D, 16>(J, tY, tU, tG, tYn, tst, e0, e1);
-  t[3] = time_row_kernel<D, 32>(J, tY, tU, tG, tYn, tst, e0, e1);
+  t[0] = time_spmv<D, 4>(J, tY, tF, e0, e1);
+  t[1] = time_spmv<D, 8>(J, tY, tF, e0, e1);
+  t[2] = time_spmv<D, 16>(J, tY, tF, e0, e1);
+  t[3] = time_spmv<D, 32>(J, tY, tF, e0, e1);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFreeAsync(buf, s);
-  cudaFreeAsync(tst, s);
   CK(e);
   CK(cudaGetLastError());
   int best = 0;
@@ -915,9 +960,7 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "hybrid upload"));
   }
-  if (J->format != SGT_FORMAT_CSR) {
-    if ((st = jalloc(J, &J->Fattr, (size_t)n * J->S)) != SGT_OK) return bail(st);
-  }
+  if ((st = jalloc(J, &J->Fattr, (size_t)n * J->S)) != SGT_OK) return bail(st);
   if (J->format == SGT_FORMAT_CSR) {
     st = tune_group(J);
     if (st != SGT_OK) return bail(st);
@@ -936,6 +979,8 @@ void sgt_job_destroy(sgt_job *J) {
     for (void *p : J->allocs) cudaFreeAsync(p, s);
   }
   delete J->st_host;
+  if (J->ev_fork) cudaEventDestroy(J->ev_fork);
+  if (J->ev_join) cudaEventDestroy(J->ev_join);
   delete J;
 }
 
@@ -999,11 +1044,59 @@ static sgt_status capture_graph(sgt_job *J, int iters, cudaGraph_t *out) {
   return SGT_OK;
 }
 
+// Node priorities of a captured iteration.  When both branches have blocks
+// waiting, the block scheduler should pick the short, latency-bound kernels
+// of the repulsion chain first (greatest priority) and fill the rest of the
+// GPU with the long, throughput-bound attractive SpMV (least priority), so
+// the chain's length hides under the SpMV.  Graphs are instantiated with
+// cudaGraphInstantiateFlagUseNodePriority so these priorities apply whatever
+// the priority of the stream they are launched into.
+static bool is_attractive_kernel(const void *f) {
+  static const void *const fs[] = {
+      (const void *)k_attr_rows<1, 4>, (const void *)k_attr_rows<1, 8>,
+      (const void *)k_attr_rows<1, 16>, (const void *)k_attr_rows<1, 32>,
+      (const void *)k_attr_rows<2, 4>, (const void *)k_attr_rows<2, 8>,
+      (const void *)k_attr_rows<2, 16>, (const void *)k_attr_rows<2, 32>,
+      (const void *)k_attr_rows<3, 4>, (const void *)k_attr_rows<3, 8>,
+      (const void *)k_attr_rows<3, 16>, (const void *)k_attr_rows<3, 32>,
+      (const void *)k_attr_ell<1>, (const void *)k_attr_ell<2>, (const void *)k_attr_ell<3>,
+      (const void *)k_attr_coo<1>, (const void *)k_attr_coo<2>, (const void *)k_attr_coo<3>};
+  for (const void *g : fs)
+    if (g == f) return true;
+  return false;
+}
+
+static sgt_status prioritise(sgt_ctx *ctx, cudaGraph_t g) {
+  size_t count = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &count));
+  std::vector<cudaGraphNode_t> nodes(count);
+  CK(cudaGraphGetNodes(g, nodes.data(), &count));
+  int least = 0, greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  for (cudaGraphNode_t nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t != cudaGraphNodeTypeKernel) continue;
+    cudaKernelNodeParams kp;
+    CK(cudaGraphKernelNodeGetParams(nd, &kp));
+    cudaLaunchAttributeValue v;
+    memset(&v, 0, sizeof(v));
+    v.priority = is_attractive_kernel(kp.func) ? least : greatest;
+    CK(cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v));
+  }
+  return SGT_OK;
+}
+
 static sgt_status instantiate(sgt_job *J, int iters, cudaGraphExec_t *exec) {
   sgt_ctx *ctx = J->ctx;
   cudaGraph_t g = nullptr;
   CKS(capture_graph(J, iters, &g));
-  cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+  sgt_status ps = prioritise(ctx, g);
+  if (ps != SGT_OK) {
+    cudaGraphDestroy(g);
+    return ps;
+  }
+  cudaError_t ie = cudaGraphInstantiateWithFlags(exec, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   CK(ie);
   return SGT_OK;
@@ -1073,7 +1166,8 @@ static sgt_status batch_build(sgt_batch *b, const std::vector<cudaGraph_t> &iter
       prev = node;
     }
   }
-  const cudaError_t ie = cudaGraphInstantiate(exec, parent, 0);
+  const cudaError_t ie =
+      cudaGraphInstantiateWithFlags(exec, parent, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(parent);
   CK(ie);
   return SGT_OK;
@@ -1101,6 +1195,7 @@ sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int i
     cudaGraph_t g = nullptr;
     st = capture_graph(jobs[k], 1, &g);
     if (st == SGT_OK) gs.push_back(g);
+    if (st == SGT_OK) st = prioritise(ctx, g);
   }
   if (st == SGT_OK) st = batch_build(b, gs, b->R, &b->exec_r);
   if (st == SGT_OK && b->R > 1) st = batch_build(b, gs, 1, &b->exec_1);
@@ -1157,8 +1252,8 @@ size_t sgt_job_footprint(const sgt_params *p, int n, long nnz) {
   b += ((size_t)n + 1) * 4;                                     // rowptr
   size_t transient = 8 * (size_t)nnz;                           // staged col/val
   if (p->format == SGT_FORMAT_CSR) {
-    b += ((size_t)nnz + 8) * 8;
-    transient = std::max(transient, 4 * np * 4);
+    b += ((size_t)nnz + 8) * 8 + np * 4;  // pairs, Fattr
+    transient = std::max(transient, 2 * np * 4);
   } else if (p->format == SGT_FORMAT_COO) {
     b += 12 * (size_t)nnz + np * 4;  // rows, cols, vals; Fattr
   } else {
@@ -1247,43 +1342,57 @@ sgt_status sgt_job_kl(sgt_job *J, double alpha, double *kl) {
   return SGT_OK;
 }
 
-sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
+}  // extern "C"
+
+template <int D>
+static sgt_status profile_iteration(sgt_job *J, cudaStream_t s, cudaEvent_t *ev) {
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaEventRecord(ev[0], s));
+  CKS(enqueue_repulsion<D>(J, s, ev));
+  CK(cudaEventRecord(ev[4], s));
+  CKS(dispatch_attractive<D>(J, s));
+  CK(cudaEventRecord(ev[5], s));
+  CKS(enqueue_combine<D>(J, s));
+  CK(cudaEventRecord(ev[6], s));
+  return SGT_OK;
+}
+
+extern "C" sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
   if (!J || !stage_ms || iters < 0) return SGT_ERR_INVALID_ARG;
   sgt_ctx *ctx = J->ctx;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
-  cudaEvent_t ev[6];
-  for (int i = 0; i < 6; i++) CK(cudaEventCreate(&ev[i]));
+  cudaEvent_t ev[7];
+  for (int i = 0; i < 7; i++) CK(cudaEventCreate(&ev[i]));
   for (int it = 0; it < iters; it++) {
-    // same kernels as the graph, bracketed per stage
-    CK(cudaEventRecord(ev[0], s));
+    // the kernels of an iteration, one stage after another on one stream
+    // (the captured iteration runs the SpMV beside the repulsion instead)
     switch (J->d) {
-      case 1: CKS(enqueue_repulsion<1>(J, s, ev)); break;
-      case 2: CKS(enqueue_repulsion<2>(J, s, ev)); break;
-      default: CKS(enqueue_repulsion<3>(J, s, ev)); break;
+      case 1: CKS(profile_iteration<1>(J, s, ev)); break;
+      case 2: CKS(profile_iteration<2>(J, s, ev)); break;
+      default: CKS(profile_iteration<3>(J, s, ev)); break;
     }
-    CK(cudaEventRecord(ev[4], s));
-    switch (J->d * 100 + J->G) {
-#define UPC(DD, GG) case DD * 100 + GG: CKS((enqueue_update<DD, GG>(J, s))); break;
-      UPC(1, 4) UPC(1, 8) UPC(1, 16) UPC(1, 32)
-      UPC(2, 4) UPC(2, 8) UPC(2, 16) UPC(2, 32)
-      UPC(3, 4) UPC(3, 8) UPC(3, 16) UPC(3, 32)
-#undef UPC
-    }
-    CK(cudaEventRecord(ev[5], s));
     CK(cudaGetLastError());
-    CK(cudaEventSynchronize(ev[5]));
+    CK(cudaEventSynchronize(ev[6]));
     float ms;
-    for (int k = 0; k < 5; k++) {
+    for (int k = 0; k < 4; k++) {
       CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
       stage_ms[k] += ms;
     }
-    CK(cudaEventElapsedTime(&ms, ev[0], ev[5]));
+    CK(cudaEventElapsedTime(&ms, ev[4], ev[6]));
+    stage_ms[4] += ms;
+    CK(cudaEventElapsedTime(&ms, ev[0], ev[6]));
     stage_ms[5] += ms;
+    CK(cudaEventElapsedTime(&ms, ev[4], ev[5]));
+    stage_ms[6] += ms;
+    CK(cudaEventElapsedTime(&ms, ev[5], ev[6]));
+    stage_ms[7] += ms;
   }
-  for (int i = 0; i < 6; i++) cudaEventDestroy(ev[i]);
+  for (int i = 0; i < 7; i++) cudaEventDestroy(ev[i]);
   return SGT_OK;
 }
+
+extern "C" {
 
 // ---------------------------------------------------------------------------
 // operators

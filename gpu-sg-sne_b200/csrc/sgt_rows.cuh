@@ -13,12 +13,13 @@
 //   KL = sum alpha p log((alpha p + FLT_MIN)/(q + FLT_MIN)), q = 1/(Z(1+d^2))
 //                                                   CU/pq.cu:61-125
 //
-// B200 structure: the default (CSR) path fuses the SpMV with the force
-// combine, the gains/momentum update and the reductions that decide the next
-// iteration's grid, so one pass streams P (8 bytes per nonzero: column and
-// value packed in an int2) and touches every per-point array once.  A group
-// of G lanes owns a row; neighbours' coordinates are gathered as one 8/16-byte
-// load.  Y is double-buffered (rows read Y while writing Ynext).
+// B200 structure: the attractive SpMV streams P once per iteration (8 bytes
+// per nonzero: column and value packed in an int2), a group of G lanes per
+// row, neighbours' coordinates gathered as one 8/16-byte load.  It depends
+// only on Y, so it runs concurrently with the latency-bound repulsion chain;
+// one combine kernel (k_row_update) then applies the force combine, the
+// gains/momentum update and the reductions that decide the next iteration's
+// grid.  Y is double-buffered (the combine reads Y while writing Ynext).
 #pragma once
 #include "sgt_common.cuh"
 #include "sgt_grid.cuh"
@@ -263,95 +264,34 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 
 
 // ---------------------------------------------------------------------------
-// Fused CSR row kernel, one row per G-lane group, launched over all rows
-// (ceil(n G / 256) blocks): the hardware refills SMs as blocks retire, so a
-// long row delays one group, not a persistent warp.  Kept lean (no loop
-// state across rows) so 48+ warps stay resident per SM.
+// Attractive term of the CSR path: one row per G-lane group, launched over
+// all rows (ceil(n G / 256) blocks; the hardware refills SMs as blocks
+// retire, so a long row delays one group, not a persistent warp).  Kept lean
+// (no loop state across rows) so 48+ warps stay resident per SM.  It reads
+// only Y and P, so the iteration runs it as a graph branch beside the
+// repulsion chain; k_row_update combines the two forces.
 // ---------------------------------------------------------------------------
 template <int D, int G>
 __global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
-k_row_fused(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
-            const typename Vec<D>::T *__restrict__ Y,
-            const typename Vec<D>::T *__restrict__ Frep_un,
-            typename Vec<D>::T *__restrict__ uY, typename Vec<D>::T *__restrict__ gains,
-            typename Vec<D>::T *__restrict__ Ynext, SgtState *st, SgtJobParams jp,
-            float4 *part_min, float4 *part_max, double *part_sum) {
-  const int n = jp.n;
+k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+            const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
+            int n) {
   const int lane = threadIdx.x % G;
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = i < n;
   float acc[3] = {0.f, 0.f, 0.f};
-  typename Vec<D>::T yi;
   if (valid) {
-    const int rs = __ldcs(&rowptr[i]), re = __ldcs(&rowptr[i + 1]);
-    yi = Y[i];
-    constexpr int U = 4;
-    for (int t0 = rs + lane; t0 < re; t0 += U * G) {
-      int2 pr[U];
-#pragma unroll
-      for (int q = 0; q < U; q++) {
-        const int t = t0 + q * G;
-        pr[q] = t < re ? __ldcs(&pairs[t]) : make_int2(i, 0);
-      }
-      typename Vec<D>::T yj[U];
-#pragma unroll
-      for (int q = 0; q < U; q++) yj[q] = __ldg(&Y[pr[q].x]);
-#pragma unroll
-      for (int q = 0; q < U; q++) attr_term<D>(yi, yj[q], __int_as_float(pr[q].y), acc);
-    }
+    const typename Vec<D>::T yi = Y[i];
+    csr_row_sum<D, G>(rowptr, pairs, Y, i, lane, yi, acc);
   }
   group_reduce<D, G>(acc);
   if (valid && lane == 0) {
-    const int iter = st->iter;
-    const float alpha = iter <= jp.early_iter ? jp.alpha0 : 1.0f;
-    const float mom = iter <= jp.mom_switch ? 0.5f : 0.8f;
-    const float Zf = (float)st->Z;
-    const typename Vec<D>::T fr = __ldcs(&Frep_un[i]);
-    typename Vec<D>::T u = __ldcs(&uY[i]), g = __ldcs(&gains[i]), yn = yi;
+    typename Vec<D>::T f;
+    if constexpr (D == 3) f.w = 0.f;
 #pragma unroll
-    for (int k = 0; k < D; k++) {
-      const float frep = comp<D>(fr, k) / Zf;
-      const float dy = alpha * acc[k] - frep;
-      float gk = comp<D>(g, k), uk = comp<D>(u, k);
-      gk = (sgn_f(dy) != sgn_f(uk)) ? (float)((double)gk + 0.2) : (float)((double)gk * 0.8);
-      if ((double)gk < 0.01) gk = (float)0.01;
-      uk = mom * uk - jp.eta * gk * dy;
-      setcomp<D>(g, k, gk);
-      setcomp<D>(u, k, uk);
-      setcomp<D>(yn, k, comp<D>(yi, k) + uk);
-    }
-    if constexpr (D == 3) { u.w = 0.f; g.w = 0.f; yn.w = 0.f; }
-    __stcs(&uY[i], u);
-    __stcs(&gains[i], g);
-    Ynext[i] = yn;
+    for (int k = 0; k < D; k++) setcomp<D>(f, k, acc[k]);
+    Fattr[i] = f;
   }
-}
-
-// ---------------------------------------------------------------------------
-// End of an iteration: min/max/sum of Ynext, the next grid decision and the
-// schedule (alpha after early_iter, momentum after iteration 250).  The row
-// kernel stays free of block-wide synchronisation.
-// ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_iter_stats(const typename Vec<D>::T *__restrict__ Ynext, SgtState *st, SgtJobParams jp,
-             float4 *part_min, float4 *part_max, double *part_sum) {
-  const int iter = st->iter;
-  const float alpha = iter <= jp.early_iter ? jp.alpha0 : 1.0f;
-  const float mom = iter <= jp.mom_switch ? 0.5f : 0.8f;
-  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  double sm[3] = {0, 0, 0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < jp.n; i += gridDim.x * blockDim.x) {
-    const typename Vec<D>::T y = Ynext[i];
-#pragma unroll
-    for (int k = 0; k < D; k++) {
-      const float v = comp<D>(y, k);
-      mn[k] = fminf(mn[k], v);
-      mx[k] = fmaxf(mx[k], v);
-      sm[k] += (double)v;
-    }
-  }
-  block_finish_stats<D>(st, jp, mn, mx, sm, part_min, part_max, part_sum, iter, alpha, mom);
 }
 
 // ---------------------------------------------------------------------------

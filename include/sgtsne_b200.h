@@ -148,8 +148,10 @@ typedef struct {
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
 sgt_status sgt_job_kl(sgt_job *job, double alpha, double *kl);
-/* Run `iters` iterations stage by stage, adding per-stage milliseconds into
-   stage_ms[8] = {bin, s2g, g2g, g2s, attractive+update, total, -, -}. */
+/* Run `iters` iterations stage by stage on one stream (the captured
+   iteration overlaps the attractive SpMV with the repulsion instead), adding
+   per-stage milliseconds into stage_ms[8] = {bin, s2g, g2g, g2s,
+   attractive+combine, total, attractive SpMV, combine}. */
 sgt_status sgt_job_profile(sgt_job *job, int iters, double *stage_ms);
 
 /* ---- batches: many independent embeddings advanced together -----------
