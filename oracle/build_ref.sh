@@ -2,7 +2,8 @@
 # Compiles the reference's own CUDA sources, where they lie under
 # /root/reference, with the test-only harnesses of oracle/ref_harness into
 # oracle/_ref/ (git-ignored; the built .so files travel with the repository
-# to the GPU box).  Used only to produce golden vectors of the reference.
+# to the GPU box).  Used only to produce golden vectors of the reference and
+# to time the reference's own GPU loop (oracle/ref_gpu_timing.py).
 set -e
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF=/root/reference/code/cuda
@@ -17,5 +18,6 @@ nvcc $FLAGS -I"$HYB/cuda" -I"$HYB" -o "$OUT/libref_hyb.so" "$HERE/ref_harness/re
 CU="$REF/SG-tSNE-CUDA/src"
 nvcc $FLAGS -I"$CU" -o "$OUT/libref_cu.so" "$HERE/ref_harness/ref_cu.cu" \
   "$CU/pq.cu" "$CU/Frep.cu" "$CU/nuconv.cu" "$CU/gridding.cu" \
-  "$CU/non_periodic_convF.cu" "$CU/non_periodic_convD.cu" "$CU/utils.cu" -lcufft
+  "$CU/non_periodic_convF.cu" "$CU/non_periodic_convD.cu" "$CU/utils.cu" \
+  "$CU/gradient_descend.cu" "$CU/compute_error.cu" -lcufft
 echo "built $OUT/libref_hyb.so $OUT/libref_cu.so"

@@ -2,18 +2,21 @@
 // (code/cuda/SG-tSNE-CUDA/src): AttractiveEstimation in COO format
 // (pq.cu:24-57) and computeFrepulsive_interp on the fixed grid
 // (Frep.cu:81-125, buffers and cuFFT plans set up as gradient_descend.cu:
-// 137-188 does).  Compiled in place from the reference tree by
-// oracle/build_ref.sh; used only to produce golden vectors.
+// 137-188 does), and the whole loop kl_minimization (gradient_descend.cu:
+// 102-282) for timing the reference's GPU path.  Compiled in place from the
+// reference tree by oracle/build_ref.sh; test and measurement use only.
 #include <cmath>
+#include <cstring>
 #include <vector>
 #include "Frep.cuh"
+#include "gradient_descend.cuh"
 #include "pq.cuh"
 #include "types.hpp"
 
+// launch shape of the reference's kernels (declared extern by its sources;
+// streamAttr/streamRep are defined by gradient_descend.cu)
 int Blocks = 592;
 int Threads = 256;
-cudaStream_t streamAttr = 0;
-cudaStream_t streamRep = 0;
 
 extern "C" int ref_cu_attractive_coo(int n, int d, int nnz, const int *rows, const int *cols,
                                      const float *vals, const float *y_dim_major, float *F) {
@@ -92,4 +95,70 @@ extern "C" float ref_cu_repulsive_fixed(int n, int d, int ng, const float *y_dim
   cudaFree(y); cudaFree(yt); cudaFree(VScat); cudaFree(PhiScat); cudaFree(VGrid);
   cudaFree(PhiGrid); cudaFree(Kc); cudaFree(Xc); cudaFree(Frep);
   return z;
+}
+
+// The reference's whole gradient-descent loop on the fixed grid
+// (kl_minimization, gradient_descend.cu:102-282) for `iters` iterations, on
+// P in format 0 (CSR: rowptr, cols, vals), 2 (COO: rows, cols, vals) or 3
+// (ELL of width ell_w, column-major, plus a COO tail).  The launch shape is
+// the one the reference's demo picks (demo_perplexity.cu:17-30: occupancy of
+// ell_spmv_kernel<float, 2>); the harness's golden-vector shape is restored
+// afterwards.  y (host, dim-major n*d) is updated in place.  Returns the
+// loop's own wall time in ms (timeInfo[7000], taken after its allocations
+// and cuFFT plans), or a negative CUDA error code.
+extern "C" double ref_cu_kl_minimization(int format, int n, int d, int nnz, int iters, int ng,
+                                         const int *rowptr_or_rows, const int *cols,
+                                         const float *vals, int ell_w,
+                                         const unsigned *ell_cols, const float *ell_vals,
+                                         int coo_n, const unsigned *coo_rows,
+                                         const unsigned *coo_cols, const float *coo_vals,
+                                         float *y_dim_major) {
+  const int saved_blocks = Blocks, saved_threads = Threads;
+  cudaOccupancyMaxPotentialBlockSize(&Blocks, &Threads, ell_spmv_kernel<float, 2>, 0, 0);
+  sparse_matrix<float> P;
+  memset(&P, 0, sizeof(P));
+  P.m = n;
+  P.n = n;
+  P.nnz = nnz;
+  P.format = format;
+  std::vector<void *> bufs;
+  auto dev = [&](const void *src, size_t bytes) {
+    void *p = nullptr;
+    cudaMallocManaged(&p, bytes);
+    cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    bufs.push_back(p);
+    return p;
+  };
+  if (format == 0 || format == 2) {
+    P.row = (int *)dev(rowptr_or_rows, sizeof(int) * (format == 0 ? (size_t)n + 1 : (size_t)nnz));
+    P.col = (int *)dev(cols, sizeof(int) * (size_t)nnz);
+    P.val = (float *)dev(vals, sizeof(float) * (size_t)nnz);
+  } else {
+    P.elements_in_rows = ell_w;
+    P.coo_size = coo_n;
+    P.ell_cols = (unsigned *)dev(ell_cols, sizeof(unsigned) * (size_t)n * ell_w);
+    P.ell_data = (float *)dev(ell_vals, sizeof(float) * (size_t)n * ell_w);
+    P.coo_row_ids = (unsigned *)dev(coo_rows, sizeof(unsigned) * (size_t)(coo_n > 0 ? coo_n : 1));
+    P.coo_col_ids = (unsigned *)dev(coo_cols, sizeof(unsigned) * (size_t)(coo_n > 0 ? coo_n : 1));
+    P.coo_data = (float *)dev(coo_vals, sizeof(float) * (size_t)(coo_n > 0 ? coo_n : 1));
+  }
+  float *y = (float *)dev(y_dim_major, sizeof(float) * (size_t)n * d);
+  tsneparams params;
+  params.d = d;
+  params.n = n;
+  params.maxIter = iters;
+  params.earlyIter = 250;
+  params.alpha = 12;
+  params.ng = ng;
+  params.format = format;
+  params.ComputeError = -1;
+  std::vector<double> time_info(7 * (size_t)(iters > 1000 ? iters : 1000) + 16, 0.0);
+  kl_minimization(y, params, P, time_info.data());
+  cudaError_t e = cudaDeviceSynchronize();
+  const double ms = time_info[7 * 1000];
+  cudaMemcpy(y_dim_major, y, sizeof(float) * (size_t)n * d, cudaMemcpyDeviceToHost);
+  for (void *p : bufs) cudaFree(p);
+  Blocks = saved_blocks;
+  Threads = saved_threads;
+  return e == cudaSuccess ? ms : -(double)e;
 }
