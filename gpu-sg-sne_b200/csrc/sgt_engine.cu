@@ -1667,6 +1667,59 @@ sgt_status sgt_csr_to_coo(sgt_ctx *ctx, int n, long nnz, const int *rowptr, unsi
 // ---------------------------------------------------------------------------
 // library entry: the flow of sgtsneCUDA (CU/sgtsne.cu:25-129)
 // ---------------------------------------------------------------------------
+// Relative L2 error of the repulsive force of the job's last iteration (the
+// numerator left in Frep over that iteration's Z) against the exact O(n^2)
+// sum at the same coordinates (Y), as the -f probe (CU/compute_error.cu:
+// 80-99) measures it.  Both forces are normalised by their own Z.
+template <int D>
+static sgt_status job_rep_error(sgt_job *J, double *out) {
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  typedef typename Vec<D>::T VT;
+  const int n = J->n;
+  double *num = nullptr, *z = nullptr;
+  CK(cudaMallocAsync(&num, sizeof(double) * (size_t)n * D, s));
+  CK(cudaMallocAsync(&z, sizeof(double) * (size_t)n, s));
+  k_frep_exact<D><<<(n + SGT_THREADS - 1) / SGT_THREADS, SGT_THREADS, 0, s>>>((const VT *)J->Y, n,
+                                                                              num, z);
+  std::vector<double> hn((size_t)n * D), hz((size_t)n);
+  std::vector<float> hf((size_t)n * J->S);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hn.data(), num, sizeof(double) * hn.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hz.data(), z, sizeof(double) * hz.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hf.data(), J->Frep, sizeof(float) * hf.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(num, s);
+  cudaFreeAsync(z, s);
+  CK(e);
+  double zx = 0;
+  for (int i = 0; i < n; i++) zx += hz[i];
+  const double ze = J->st_host->Z;
+  double err2 = 0, nrm2 = 0;
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < D; k++) {
+      const double fx = hn[(size_t)i * D + k] / zx, fe = (double)hf[(size_t)i * J->S + k] / ze;
+      err2 += (fx - fe) * (fx - fe);
+      nrm2 += fx * fx;
+    }
+  *out = nrm2 > 0 ? std::sqrt(err2 / nrm2) : 0.0;
+  return SGT_OK;
+}
+
+extern "C" sgt_status sgt_job_repulsive_error(sgt_job *J, double *rel_err) {
+  if (!J || !rel_err) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  if (J->host_iter < 1)
+    return fail(ctx, SGT_ERR_INVALID_ARG, "the job has not run an iteration since set_y");
+  CK(cudaSetDevice(ctx->device));
+  switch (J->d) {
+    case 1: return job_rep_error<1>(J, rel_err);
+    case 2: return job_rep_error<2>(J, rel_err);
+    default: return job_rep_error<3>(J, rel_err);
+  }
+}
+
 extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const int *col,
                                 const float *val, const sgt_params *params, const float *y_in,
                                 float *y_out, double *time_info) {
@@ -1675,8 +1728,6 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   sgt_params p = *params;
   p.n = n;
   if (p.d < 1 || p.d > 3) return fail(ctx, SGT_ERR_UNSUPPORTED, "d must be 1, 2 or 3");
-  if (p.compute_error > 0)
-    return fail(ctx, SGT_ERR_UNSUPPORTED, "compute_error is not implemented by this engine");
   // default h per dimension (CU/sgtsne.cu:29-40)
   if (p.h <= 0) p.h = p.d == 1 ? 0.5f : (p.d == 2 ? 0.7f : 1.2f);
   CK(cudaSetDevice(ctx->device));
@@ -1727,7 +1778,26 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   }
   sgt_status st = sgt_job_set_y(J, ysrc, SGT_LAYOUT_DIM_MAJOR, 0);
   const auto t1 = std::chrono::steady_clock::now();
-  if (st == SGT_OK) st = sgt_job_run(J, p.max_iter);
+  std::vector<double> errs;
+  if (st == SGT_OK && p.compute_error > 0) {
+    // every 10th iteration (0, 10, 20, ...) the error of its repulsive force
+    // against the exact sum (CU/gradient_descend.cu:203-213)
+    for (int it = 0; it < p.max_iter && st == SGT_OK;) {
+      if (it % 10 == 0) {
+        st = sgt_job_run(J, 1);
+        double e = 0;
+        if (st == SGT_OK) st = sgt_job_repulsive_error(J, &e);
+        errs.push_back(e);
+        it++;
+      } else {
+        const int k = std::min(10 - it % 10, p.max_iter - it);
+        st = sgt_job_run(J, k);
+        it += k;
+      }
+    }
+  } else if (st == SGT_OK) {
+    st = sgt_job_run(J, p.max_iter);
+  }
   if (st == SGT_OK) st = sgt_job_get_y(J, y_out, SGT_LAYOUT_DIM_MAJOR, 0, 1);
   const auto t2 = std::chrono::steady_clock::now();
   if (st == SGT_OK && time_info) {
@@ -1741,6 +1811,20 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
     st = sgt_job_get_info(J, &info);
     if (st == SGT_OK && (info.error_flags & SGT_EFLAG_NONFINITE))
       st = fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates during the iterations");
+  }
+  if (st == SGT_OK && p.compute_error > 0) {
+    // appended to errorInfo.txt in the working directory, one line per run,
+    // as the reference does (CU/gradient_descend.cu:254-266; the reference
+    // writes the values only when the file already exists, this engine
+    // always writes them)
+    FILE *f = fopen("errorInfo.txt", "a");
+    if (!f) {
+      st = fail(ctx, SGT_ERR_INVALID_ARG, "cannot append to errorInfo.txt");
+    } else {
+      for (double e : errs) fprintf(f, "%g ", e);
+      fprintf(f, "\n");
+      fclose(f);
+    }
   }
   sgt_job_destroy(J);
   return st;

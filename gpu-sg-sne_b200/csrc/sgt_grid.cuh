@@ -665,3 +665,58 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
     }
   }
 }
+
+// ---------------------------------------------------------------------------
+// Exact O(n^2) repulsion, for the -f error probe (CU/compute_error.cu:8-57):
+// num_i = sum_{j != i} (y_i - y_j)/(1 + |y_i - y_j|^2)^2 and
+// z_i = sum_{j != i} 1/(1 + |y_i - y_j|^2).  One point per thread; the other
+// points stream through shared memory in tiles of SGT_THREADS, summed in
+// FP32 within a tile and in FP64 across tiles.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_frep_exact(const typename Vec<D>::T *__restrict__ Y, int n, double *__restrict__ num,
+             double *__restrict__ z) {
+  __shared__ float ts[SGT_THREADS][D];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float yi[3] = {0.f, 0.f, 0.f};
+  if (i < n) {
+    const typename Vec<D>::T v = Y[i];
+#pragma unroll
+    for (int k = 0; k < D; k++) yi[k] = comp<D>(v, k);
+  }
+  double an[3] = {0, 0, 0}, az = 0;
+  for (int j0 = 0; j0 < n; j0 += SGT_THREADS) {
+    const int j = j0 + threadIdx.x;
+    if (j < n) {
+      const typename Vec<D>::T v = Y[j];
+#pragma unroll
+      for (int k = 0; k < D; k++) ts[threadIdx.x][k] = comp<D>(v, k);
+    }
+    __syncthreads();
+    const int m = min(SGT_THREADS, n - j0);
+    float fn[3] = {0.f, 0.f, 0.f}, fz = 0.f;
+    for (int t = 0; t < m; t++) {
+      if (j0 + t == i) continue;
+      float df[3], d2 = 0.f;
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        df[k] = yi[k] - ts[t][k];
+        d2 += df[k] * df[k];
+      }
+      const float q = 1.0f / (1.0f + d2);
+      fz += q;
+#pragma unroll
+      for (int k = 0; k < D; k++) fn[k] += q * q * df[k];
+    }
+    az += fz;
+#pragma unroll
+    for (int k = 0; k < D; k++) an[k] += fn[k];
+    __syncthreads();
+  }
+  if (i < n) {
+    z[i] = az;
+#pragma unroll
+    for (int k = 0; k < D; k++) num[(long)i * D + k] = an[k];
+  }
+}

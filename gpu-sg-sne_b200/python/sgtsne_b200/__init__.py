@@ -86,6 +86,7 @@ SIGNATURES = {
     "sgt_job_get_info": (_i, [_vp, C.POINTER(JobInfo)]),
     "sgt_job_kl": (_i, [_vp, _d, C.POINTER(_d)]),
     "sgt_job_profile": (_i, [_vp, _i, _vp]),
+    "sgt_job_repulsive_error": (_i, [_vp, C.POINTER(_d)]),
     "sgt_batch_create": (_i, [_vp, _i, C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "sgt_batch_run": (_i, [_vp, _i]),
     "sgt_batch_destroy": (None, [_vp]),
@@ -296,6 +297,11 @@ class Job:
     def kl(self, alpha=-1.0):
         out = C.c_double()
         self.ctx.check(self.lib.sgt_job_kl(self.h, float(alpha), C.byref(out)), "kl")
+        return out.value
+
+    def repulsive_error(self):
+        out = C.c_double()
+        self.ctx.check(self.lib.sgt_job_repulsive_error(self.h, C.byref(out)), "repulsive_error")
         return out.value
 
     def profile(self, iters):

@@ -153,6 +153,14 @@ sgt_status sgt_job_kl(sgt_job *job, double alpha, double *kl);
    per-stage milliseconds into stage_ms[8] = {bin, s2g, g2g, g2s,
    attractive+combine, total, attractive SpMV, combine}. */
 sgt_status sgt_job_profile(sgt_job *job, int iters, double *stage_ms);
+/* Relative L2 error ||F_exact - F|| / ||F_exact|| of the repulsive force of
+   the job's last iteration against the exact O(n^2) sum at the same
+   coordinates, both normalised by their own Z.  Replaces computeError
+   (CU/compute_error.cu:80-99), the probe behind the -f option; costs O(n^2)
+   work.  sgt_embed with compute_error > 0 calls it every 10th iteration
+   (0, 10, 20, ...) and appends the values to errorInfo.txt in the working
+   directory, one line per run (CU/gradient_descend.cu:203-213, 254-266). */
+sgt_status sgt_job_repulsive_error(sgt_job *job, double *rel_err);
 
 /* ---- batches: many independent embeddings advanced together -----------
  * No counterpart in the reference, which runs one embedding per process

@@ -341,3 +341,45 @@ def test_relayout_is_transparent(torch, ctx):
         assert rel(again, out[every]) <= 1e-4
         job.close()
     assert rel(out[10], out[0]) <= 1e-4
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_repulsive_error_probe(torch, ctx, oracle, d):
+    """sgt_job_repulsive_error (the -f probe of CU/compute_error.cu:80-99):
+    after one iteration from Y0 the job's repulsive force was computed at the
+    centred Y0, so the probe must equal rel-L2(F_interp(Y0), F_exact(Y0)),
+    F_exact from the oracle's FP64 direct sum, within 2 % of its value."""
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=3000, k=12, seed=30 + d)
+    n = len(rp) - 1
+    Y0 = coords("clusters", n, d, seed=31 + d) * np.float32(0.2)
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    p = S.default_params(d=d, format=S.FORMAT_CSR, h=h)
+    job = S.Job(ctx, p, rp, col, val.astype(np.float32), device_mem=False)
+    job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+    job.run(1)
+    e_job = job.repulsive_error()
+    job.close()
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    ctx.repulsive(n, d, h, 0, dev(torch, Y0), S.LAYOUT_POINT_MAJOR, f)
+    Fx, _ = oracle.repulsive_exact(Y0.astype(np.float64))
+    e_ref = rel(f.cpu().numpy().reshape(n, d), Fx)
+    assert 0 < e_job < 0.5  # the interpolation error itself is ~1e-2..1e-1 here
+    assert abs(e_job - e_ref) <= 0.02 * e_ref
+
+
+def test_embed_compute_error_writes_error_info(torch, ctx, tmp_path, monkeypatch):
+    """sgt_embed with compute_error = 1 appends one line of max_iter/10
+    errors to errorInfo.txt, as the reference's -f option does."""
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=1500, k=10, seed=44)
+    monkeypatch.chdir(tmp_path)
+    p = S.default_params(d=2, max_iter=35, early_iter=20, format=S.FORMAT_CSR)
+    p.compute_error = 1
+    ctx.embed(rp, col, val.astype(np.float32), p)
+    ctx.embed(rp, col, val.astype(np.float32), p)
+    lines = (tmp_path / "errorInfo.txt").read_text().splitlines()
+    assert len(lines) == 2
+    errs = [float(x) for x in lines[0].split()]
+    assert len(errs) == 4  # iterations 0, 10, 20, 30
+    assert all(0 < e < 0.5 for e in errs)
