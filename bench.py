@@ -209,8 +209,8 @@ def initial_state(n, d, seed):
 
 
 def build_problem(args, dev, ctx):
-    """kNN on the device, lambda bisection through the engine, host
-    symmetrisation; returns (X, srp, sc, sv)."""
+    """kNN on the device, then lambda bisection and (P + P^T)/(2n) through
+    the engine on the device; returns (X, srp, sc, sv) on the host."""
     import torch
 
     import sgtsne_b200 as S
@@ -219,13 +219,15 @@ def build_problem(args, dev, ctx):
     k = idx.shape[1]
     rp_knn = torch.arange(0, (n + 1) * k, k, dtype=torch.int32, device=dev)
     vals = d2.reshape(-1).contiguous().clone()
+    col = idx.reshape(-1).to(torch.int32).contiguous()
     torch.cuda.synchronize(dev)  # torch's writes complete before the engine reads
     ctx.lambda_bisect(n, rp_knn, vals, 10.0, 1)
-    rp_h = rp_knn.cpu().numpy()
-    col_h = idx.reshape(-1).cpu().numpy().astype(np.int32)
-    val_h = vals.cpu().numpy()
-    srp, sc, sv = S.symmetrize(rp_h, col_h, val_h, 1.0 / (2 * n))
-    return X, srp, sc, sv
+    nnz = int(col.numel())
+    srp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    sc = torch.empty(2 * nnz, dtype=torch.int32, device=dev)
+    sv = torch.empty(2 * nnz, dtype=torch.float32, device=dev)
+    m = ctx.symmetrize(n, nnz, rp_knn, col, vals, 1.0 / (2 * n), srp, sc, sv)
+    return X, srp.cpu().numpy(), sc[:m].cpu().numpy(), sv[:m].cpu().numpy()
 
 
 def run_params(S, args):

@@ -8,6 +8,7 @@
 // the same kernels on caller buffers for parity tests and for callers that
 // drive the loop themselves.
 #include "../../include/sgtsne_b200.h"
+#include "sgt_internal.h"
 #include "sgt_common.cuh"
 #include "sgt_fft.cuh"
 #include "sgt_grid.cuh"
@@ -92,6 +93,9 @@ static sgt_status fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) {
   if (ctx) ctx->err = msg;
   return s;
 }
+cudaStream_t sgti_stream(sgt_ctx *ctx) { return ctx->stream; }
+int sgti_device(sgt_ctx *ctx) { return ctx->device; }
+sgt_status sgti_fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) { return fail(ctx, s, msg); }
 #define CK(call)                                                              \
   do {                                                                        \
     cudaError_t e_ = (call);                                                  \
@@ -1735,35 +1739,43 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   const auto t0 = std::chrono::steady_clock::now();
   CKS(check_csr(ctx, n, rowptr, col));
   const long nnz = rowptr[n];
-  std::vector<float> v(val, val + nnz);
-  // lambda rescaling unless lambda == 1 (CU/sgtsne.cu:51-54)
-  if (p.lambda != 1.0f) {
-    int *drp = nullptr;
-    float *dv = nullptr;
-    CK(cudaMallocAsync(&drp, sizeof(int) * (n + 1), s));
-    CK(cudaMallocAsync(&dv, sizeof(float) * nnz, s));
-    CK(cudaMemcpyAsync(drp, rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(dv, v.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
-    sgt_status ls = sgt_lambda_bisect(ctx, n, drp, dv, p.lambda, p.lambda_dist, nullptr);
-    if (ls == SGT_OK) {
-      CK(cudaMemcpyAsync(v.data(), dv, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-    }
-    cudaFreeAsync(drp, s);
-    cudaFreeAsync(dv, s);
-    if (ls != SGT_OK) return ls;
-    if (p.drop_leaf)
-      for (int r = 0; r < n; r++)
-        if (rowptr[r + 1] - rowptr[r] == 1) v[rowptr[r]] = 0.f;
+  // P prepared on the device: lambda rescaling unless lambda == 1
+  // (CU/sgtsne.cu:51-54), leaves dropped, (P + P^T)/(2n) (CU/sgtsne.cu:64-65)
+  int *drp = nullptr, *dc = nullptr, *srp = nullptr, *sc = nullptr;
+  float *dv = nullptr, *sv = nullptr;
+  auto release = [&]() {
+    for (void *q : {(void *)drp, (void *)dc, (void *)dv, (void *)srp, (void *)sc, (void *)sv})
+      if (q) cudaFreeAsync(q, s);
+  };
+  cudaError_t ae = cudaMallocAsync(&drp, sizeof(int) * ((size_t)n + 1), s);
+  if (ae == cudaSuccess) ae = cudaMallocAsync(&dc, sizeof(int) * (size_t)std::max(nnz, 1L), s);
+  if (ae == cudaSuccess) ae = cudaMallocAsync(&dv, sizeof(float) * (size_t)std::max(nnz, 1L), s);
+  if (ae == cudaSuccess) ae = cudaMallocAsync(&srp, sizeof(int) * ((size_t)n + 1), s);
+  if (ae == cudaSuccess) ae = cudaMallocAsync(&sc, sizeof(int) * (size_t)std::max(2 * nnz, 1L), s);
+  if (ae == cudaSuccess) ae = cudaMallocAsync(&sv, sizeof(float) * (size_t)std::max(2 * nnz, 1L), s);
+  if (ae == cudaSuccess) ae = cudaMemcpyAsync(drp, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, s);
+  if (ae == cudaSuccess) ae = cudaMemcpyAsync(dc, col, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s);
+  if (ae == cudaSuccess) ae = cudaMemcpyAsync(dv, val, sizeof(float) * (size_t)nnz, cudaMemcpyHostToDevice, s);
+  if (ae != cudaSuccess) {
+    release();
+    return fail(ctx, ae == cudaErrorMemoryAllocation ? SGT_ERR_NO_MEMORY : SGT_ERR_CUDA,
+                std::string("sgt_embed: staging P: ") + cudaGetErrorString(ae));
   }
-  // symmetrise (P + P^T)/(2n) (CU/sgtsne.cu:64-65)
+  sgt_status ps = SGT_OK;
+  if (p.lambda != 1.0f) {
+    ps = sgt_lambda_bisect(ctx, n, drp, dv, p.lambda, p.lambda_dist, nullptr);
+    if (ps == SGT_OK && p.drop_leaf) {
+      k_drop_leaf<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(n, drp, dv);
+      if (cudaGetLastError() != cudaSuccess) ps = fail(ctx, SGT_ERR_CUDA, "sgt_embed: drop leaves");
+    }
+  }
   long snnz = 0;
-  CKS(sgt_symmetrize(n, rowptr, col, v.data(), 1.0f / (2.0f * n), nullptr, nullptr, nullptr, &snnz));
-  std::vector<int> srp(n + 1), sc(snnz);
-  std::vector<float> sv(snnz);
-  CKS(sgt_symmetrize(n, rowptr, col, v.data(), 1.0f / (2.0f * n), srp.data(), sc.data(), sv.data(), &snnz));
+  if (ps == SGT_OK)
+    ps = sgt_symmetrize_device(ctx, n, nnz, drp, dc, dv, 1.0f / (2.0f * n), srp, sc, sv, &snnz);
   sgt_job *J = nullptr;
-  CKS(sgt_job_create(ctx, &p, n, srp.data(), sc.data(), sv.data(), 0, &J));
+  if (ps == SGT_OK) ps = sgt_job_create(ctx, &p, n, srp, sc, sv, 1, &J);
+  release();
+  if (ps != SGT_OK) return ps;
   // initial coordinates: given, or 1e-4 N(0,1) as generateRandomGaussianCoord
   // (CU/utils.cu:185-193), dim-major
   std::vector<float> y0;

@@ -1,0 +1,13 @@
+// sgt_internal.h -- context accessors shared by the engine's translation
+// units (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/sgtsne_b200.h"
+
+cudaStream_t sgti_stream(sgt_ctx *ctx);
+int sgti_device(sgt_ctx *ctx);
+// records msg as the context's last error and returns s
+sgt_status sgti_fail(sgt_ctx *ctx, sgt_status s, const std::string &msg);

@@ -155,3 +155,12 @@ __global__ void k_validate_csr(int n, const int *__restrict__ rowptr,
       }
   }
 }
+
+// rows with a single entry lose it (dropLeafEdge of the lambda rescaling,
+// CU/graph_rescaling.cu:91, called with params.dropLeaf at CU/sgtsne.cu:54):
+// the value becomes 0
+__global__ void k_drop_leaf(int n, const int *__restrict__ rowptr, float *__restrict__ val) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    if (rowptr[r + 1] - rowptr[r] == 1) val[rowptr[r]] = 0.f;
+}
+

@@ -114,6 +114,7 @@ SIGNATURES = {
     "sgt_ell_width": (_i, [_i, _vp]),
     "sgt_csr_to_hybrid": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_symmetrize": (_i, [_i, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
+    "sgt_symmetrize_device": (_i, [_vp, _i, _l, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
 }
 
 _LIB = None
@@ -235,6 +236,16 @@ class Context:
     def perplexity(self, n, k, dist, perp, p, beta=None):
         self.check(self.lib.sgt_perplexity(self.h, n, k, _ptr(dist), float(perp), _ptr(p),
                                            _ptr(beta)), "perplexity")
+
+    def symmetrize(self, n, nnz, rowptr, col, val, scale, out_rowptr, out_col, out_val):
+        """(P + P^T) * scale on the device; out_col/out_val hold 2 nnz.
+        Returns the output nnz."""
+        out = C.c_long()
+        self.check(self.lib.sgt_symmetrize_device(self.h, int(n), int(nnz), _ptr(rowptr),
+                                                  _ptr(col), _ptr(val), float(scale),
+                                                  _ptr(out_rowptr), _ptr(out_col), _ptr(out_val),
+                                                  C.byref(out)), "symmetrize_device")
+        return out.value
 
     def csr_to_coo(self, n, nnz, rowptr, rows):
         self.check(self.lib.sgt_csr_to_coo(self.h, n, nnz, _ptr(rowptr), _ptr(rows)), "csr_to_coo")

@@ -4,8 +4,8 @@ the continuous-batching server), each beside its plain form (the same jobs
 run one after another through sgt_job_run).
 
 Used by bench.py.  P of every instance is built on the device (exact kNN
-with fp32 matrix products, lambda bisection through the engine) and
-symmetrised on the host, as for the single-embedding benchmark.
+with fp32 matrix products, lambda bisection and symmetrisation through the
+engine), as for the single-embedding benchmark.
 """
 from __future__ import annotations
 
@@ -18,17 +18,20 @@ from . import workloads as W
 
 def _csr_from_knn(ctx, idx, d2, lam, dev):
     import torch
-
-    from . import symmetrize
     n, k = idx.shape
     rp = torch.arange(0, (n + 1) * k, k, dtype=torch.int32, device=dev)
     vals = d2.reshape(-1).contiguous().clone()
+    col = idx.reshape(-1).to(torch.int32).contiguous()
     # the engine works on its own stream: the tensors torch just wrote on
     # its stream must be complete before the engine reads them
     torch.cuda.synchronize(dev)
     ctx.lambda_bisect(n, rp, vals, float(lam), 1)
-    return symmetrize(rp.cpu().numpy(), idx.reshape(-1).cpu().numpy().astype(np.int32),
-                      vals.cpu().numpy(), 1.0 / (2 * n))
+    nnz = n * k
+    srp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    sc = torch.empty(2 * nnz, dtype=torch.int32, device=dev)
+    sv = torch.empty(2 * nnz, dtype=torch.float32, device=dev)
+    m = ctx.symmetrize(n, nnz, rp, col, vals, 1.0 / (2 * n), srp, sc, sv)
+    return srp.cpu().numpy(), sc[:m].cpu().numpy(), sv[:m].cpu().numpy()
 
 
 def batched_instances(ctx, count, seed, dev, n_lo=2000, n_hi=200000, k=30):

@@ -331,6 +331,16 @@ sgt_status sgt_csr_to_hybrid(int n, const int *rowptr, const int *col,
                              unsigned *coo_cols, float *coo_vals,
                              long *coo_size);
 
+/* The same on the device: device arrays, out_col/out_val sized 2*nnz (an
+   upper bound), out_rowptr n+1; *out_nnz receives the count (synchronises
+   the context's stream).  Bit-identical to sgt_symmetrize.  n <= 2^24,
+   nnz <= 2^30.  Replaces the cuSPARSE csrgeam path of SymmetrizeMatrix
+   (CU/graph_rescaling.cu:266-398). */
+sgt_status sgt_symmetrize_device(sgt_ctx *ctx, int n, long nnz, const int *rowptr,
+                                 const int *col, const float *val, float scale,
+                                 int *out_rowptr, int *out_col, float *out_val,
+                                 long *out_nnz);
+
 /* (P + P^T) * scale with sorted columns per row (CU/graph_rescaling.cu:266-398
    uses scale 1/(2n)).  Host arrays.  Call with out_col == NULL to get
    *out_nnz, then again with out arrays of that size. */

@@ -383,3 +383,54 @@ def test_embed_compute_error_writes_error_info(torch, ctx, tmp_path, monkeypatch
     errs = [float(x) for x in lines[0].split()]
     assert len(errs) == 4  # iterations 0, 10, 20, 30
     assert all(0 < e < 0.5 for e in errs)
+
+
+@pytest.mark.parametrize("case", ["knn", "ragged"])
+def test_symmetrize_device_bit_exact(torch, ctx, case):
+    """sgt_symmetrize_device against the host sgt_symmetrize: same rowptr,
+    columns and value bits.  'knn': rows of 15 neighbours in distance order
+    (unsorted columns); 'ragged': empty rows, single-entry rows and repeated
+    columns inside a row."""
+    import sgtsne_b200 as S
+    rng = np.random.default_rng(71)
+    if case == "knn":
+        from sgtsne_b200 import workloads as W
+        X, _ = W.gmm_isotropic(5000, 20, 6, 16.0, 9)
+        idx, d2 = W.knn_numpy(X, 15)
+        rp, col, val = W.knn_csr(idx, d2)
+        val = (val / val.max()).astype(np.float32)
+    else:
+        n = 3000
+        lens = rng.integers(0, 9, n)
+        lens[rng.integers(0, n, 300)] = 0
+        lens[rng.integers(0, n, 300)] = 1
+        rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+        col = rng.integers(0, n, int(rp[-1])).astype(np.int32)
+        dup = rng.integers(0, int(rp[-1]) - 1, 400)
+        col[dup + 1] = col[dup]  # repeats (some cross a row end: harmless)
+        val = rng.random(int(rp[-1])).astype(np.float32)
+    n = len(rp) - 1
+    nnz = int(rp[-1])
+    hrp, hc, hv = S.symmetrize(rp, col, val, 1.0 / (2 * n))
+    orp = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    oc = torch.empty(2 * nnz, dtype=torch.int32, device="cuda")
+    ov = torch.empty(2 * nnz, dtype=torch.float32, device="cuda")
+    m = ctx.symmetrize(n, nnz, dev(torch, rp), dev(torch, col), dev(torch, val), 1.0 / (2 * n),
+                       orp, oc, ov)
+    assert m == len(hc)
+    assert np.array_equal(orp.cpu().numpy(), hrp)
+    assert np.array_equal(oc[:m].cpu().numpy(), hc)
+    assert np.array_equal(ov[:m].cpu().numpy().view(np.uint32), hv.view(np.uint32))
+
+
+def test_symmetrize_device_rejects_bad_column(torch, ctx):
+    import sgtsne_b200 as S
+    rp = np.array([0, 2, 3], np.int32)
+    col = np.array([1, 5, 0], np.int32)  # 5 >= n
+    val = np.ones(3, np.float32)
+    orp = torch.empty(3, dtype=torch.int32, device="cuda")
+    oc = torch.empty(6, dtype=torch.int32, device="cuda")
+    ov = torch.empty(6, dtype=torch.float32, device="cuda")
+    with pytest.raises(S.SgtError) as e:
+        ctx.symmetrize(2, 3, dev(torch, rp), dev(torch, col), dev(torch, val), 0.25, orp, oc, ov)
+    assert e.value.status == 1
