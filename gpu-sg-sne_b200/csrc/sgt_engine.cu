@@ -78,7 +78,8 @@ struct sgt_job {
   int nb_pts = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0,
       nb_upd = 0, nb_part = 0;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // the two branches of an iteration
-  size_t smem_s2g = 0, smem_fft1 = 0, smem_fft2 = 0;
+  size_t smem_s2g = 0, smem_s2g8 = 0, smem_fft1 = 0, smem_fft2 = 0;
+  int nb_s2g8 = 0;  // 3-D tiles of 8 cells
   cudaGraphExec_t gexec = nullptr;        // one iteration
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
@@ -283,12 +284,17 @@ static sgt_status job_shapes(sgt_job *J) {
   const int nsm = ctx->nsm;
   int occ = 0;
   J->nb_pts = grid_blocks(nsm, 4);
-  const int T = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  constexpr int T = D == 1 ? 512 : (D == 2 ? 32 : 16);
   const int R = T + 3;
   J->smem_s2g = sizeof(float) * (D + 1) * (size_t)(D == 1 ? R : (D == 2 ? R * R : R * R * R));
-  CK(cudaFuncSetAttribute(k_s2g<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_s2g));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g<D>, SGT_THREADS, J->smem_s2g));
+  CK(cudaFuncSetAttribute(k_s2g<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_s2g));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g<D, T>, SGT_THREADS, J->smem_s2g));
   J->nb_s2g = grid_blocks(nsm, occ);
+  if constexpr (D == 3) {
+    J->smem_s2g8 = sizeof(float) * 4 * 11 * 11 * 11;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g<3, 8>, SGT_THREADS, J->smem_s2g8));
+    J->nb_s2g8 = grid_blocks(nsm, occ);
+  }
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g_cell<D>, SGT_THREADS, 0));
   J->nb_s2gc = grid_blocks(nsm, occ);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2s<D>, SGT_THREADS, 0));
@@ -324,6 +330,7 @@ static sgt_status job_shapes(sgt_job *J) {
   const int cap = (int)std::max(1L, ((long)J->n + 255) / 256);
   J->nb_pts = std::min(J->nb_pts, cap);
   J->nb_s2g = std::min(J->nb_s2g, cap);
+  J->nb_s2g8 = std::min(J->nb_s2g8, cap);
   J->nb_s2gc = std::min(J->nb_s2gc, cap);
   J->nb_g2s = std::min(J->nb_g2s, cap);
   J->nb_row = std::min(J->nb_row, cap);
@@ -370,7 +377,7 @@ static sgt_status job_alloc(sgt_job *J) {
   if (D >= 2) CKS(jalloc(J, &J->W, 3 * plane));
   CKS(jalloc(J, &J->tile_count, SGT_HIST_MAX));
   CKS(jalloc(J, &J->cursor, SGT_HIST_MAX));
-  J->jp.chunk_cap = J->n / 1024 + SGT_HIST_MAX + 16;
+  J->jp.chunk_cap = J->n / 256 + SGT_HIST_MAX + 16;  // 3-D chunks may hold 256 points
   CKS(jalloc(J, &J->chunks, (size_t)J->jp.chunk_cap));
   J->jp.mmax = M;
   J->jp.tile_cap = SGT_HIST_MAX;
@@ -478,7 +485,10 @@ static sgt_status enqueue_repulsion_rest(sgt_job *J, cudaStream_t s, cudaEvent_t
                                                      J->sorted);
   if (ev) CK(cudaEventRecord(ev[1], s));
   // tile mode and cell mode: the kernel of the other mode returns at once
-  k_s2g<D><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+  constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  k_s2g<D, TT><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+  if constexpr (D == 3)
+    k_s2g<3, 8><<<J->nb_s2g8, SGT_THREADS, J->smem_s2g8, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
   k_s2g_cell<D><<<J->nb_s2gc, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
   if (ev) CK(cudaEventRecord(ev[2], s));
   CKS(enqueue_g2g<D>(J, s));
@@ -1250,7 +1260,7 @@ size_t sgt_job_footprint(const sgt_params *p, int n, long nnz) {
   if (D >= 3) { nodes *= nmax; plane *= M; }
   b += 2 * nodes * (D == 1 ? 2 : 4) * 4;                       // V, Phi
   if (D >= 2) b += 3 * plane * 8;                               // FFT planes
-  b += 2 * 4096 * 4 + ((size_t)n / 1024 + 4096 + 16) * 16;       // tiles, chunks
+  b += 2 * 4096 * 4 + ((size_t)n / 256 + 4096 + 16) * 16;        // tiles, chunks
   const size_t parts = std::max<size_t>(148 * 16, ((size_t)n * 32 + 255) / 256);
   b += parts * (16 + 16 + 32 + 8 + 8) + 1024;                   // partials, state
   b += ((size_t)n + 1) * 4;                                     // rowptr

@@ -80,7 +80,10 @@ __device__ void sgt_finalize_grid(SgtState *st, const SgtJobParams &jp,
   // enough points each that one block reduction per chunk of a cell is
   // cheaper than shared-memory atomics that all land on a few nodes
   const bool cell_mode = ncell <= SGT_HIST_MAX && (long)jp.n >= 64L * ncell;
-  const int T = cell_mode ? 1 : (D == 1 ? 512 : (D == 2 ? 32 : 16));
+  // 3-D tiles of 8 cells while the tile count fits the tile arrays: a
+  // (8+3)^3 x 4-channel shared accumulator is 21 KB (a 16-cell tile: 110 KB),
+  // so each chunk zeroes and flushes 5x fewer nodes and more CTAs fit an SM
+  const int T = cell_mode ? 1 : (D == 1 ? 512 : (D == 2 ? 32 : (cells <= 128 ? 8 : 16)));
   const int td = (cells + T - 1) / T;
   int nt = td;
   if (D >= 2) nt *= td;
@@ -269,9 +272,12 @@ k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
            int *__restrict__ cursor, int4 *__restrict__ chunks, int nblk) {
   const int ntiles = st->ntiles;
   // chunk length: about two chunks per persistent CTA, at least 1024 points
+  // (256 in 3-D, where a point costs 64 nodes and small jobs need more
+  // chunks than they have 1024-point runs)
   int chunk = (jp.n + 2 * nblk - 1) / (2 * nblk);
   chunk = ((chunk + 255) / 256) * 256;
-  if (chunk < 1024) chunk = 1024;
+  const int cmin = jp.d == 3 ? 256 : 1024;
+  if (chunk < cmin) chunk = cmin;
   const int per = (ntiles + 1023) / 1024;  // <= 4
   int cnt[4], cpt[4];
   int mysum = 0, mych = 0;
@@ -397,13 +403,15 @@ __device__ __forceinline__ void sgt_point_stencil(const float4 &rec,
   }
 }
 
-template <int D>
+// TT: the tile edge this instance handles; the instances of the other tile
+// edges (and k_s2g_cell in cell mode) return at once.
+template <int D, int TT>
 __global__ void __launch_bounds__(SGT_THREADS)
 k_s2g(const float4 *__restrict__ sorted, SgtState *st,
       const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
   extern __shared__ float acc[];  // [D+1][R^D]
   const int T = st->T, td = st->tiles_dim, N = st->N, nch = st->nchunks;
-  if (T == 1) return;  // cell mode: k_s2g_cell does the work
+  if (T != TT) return;
   const float maxy = st->maxy, scale = st->scale;
   // charges are taken about the middle of the grid: F and Z are invariant to
   // the origin of y, and |y - c| <= maxy/2 halves the cancellation in
@@ -425,6 +433,66 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
     if (D >= 3) o[2] = (ch.x / (td * td)) * T;
     for (int e = threadIdx.x; e < m * RD; e += blockDim.x) acc[e] = 0.f;
     __syncthreads();
+    if constexpr (D == 3) {
+      // The lanes of a warp share one point at a time, each owning 2 of its
+      // 64 stencil nodes, so the 32 atomics of an instruction go to 32
+      // distinct nodes.  (With a point per thread, the points of a cluster
+      // sit in few cells and all lanes of a warp collide on the same nodes.)
+      // Points come 32 per warp in one coalesced load; each lane computes
+      // the stencil of its own point and the warp hands the stencils round
+      // by shuffles.
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+      const int a0 = lane & 3, a1 = (lane >> 2) & 3, a2b = lane >> 4;
+      for (int j0 = ch.y + 32 * wid; j0 < ch.y + ch.z; j0 += 32 * nw) {
+        const int jm = min(32, ch.y + ch.z - j0);
+        int f[3] = {0, 0, 0};
+        float w[3][4], ys[3];
+        int node0 = -1;  // this lane's point: base node in the tile, -1 if none
+        if (lane < jm) {
+          const float4 rec = sorted[j0 + lane];
+          sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
+          const int l0 = f[0] - o[0], l1 = f[1] - o[1], l2 = f[2] - o[2];
+          if ((unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T &&
+              (unsigned)l2 < (unsigned)T) {
+            node0 = l0 + R * (l1 + R * l2);
+          } else {  // the sort and the binning disagree: skip the point
+            atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            ys[k] = 0.f;
+#pragma unroll
+            for (int a = 0; a < 4; a++) w[k][a] = 0.f;
+          }
+        }
+        for (int t = 0; t < jm; t++) {
+          const int nb = __shfl_sync(0xffffffffu, node0, t);
+          float wx[4], wy4[4], wz4[4], qc[3];
+#pragma unroll
+          for (int a = 0; a < 4; a++) {
+            wx[a] = __shfl_sync(0xffffffffu, w[0][a], t);
+            wy4[a] = __shfl_sync(0xffffffffu, w[1][a], t);
+            wz4[a] = __shfl_sync(0xffffffffu, w[2][a], t);
+          }
+#pragma unroll
+          for (int k = 0; k < 3; k++) qc[k] = __shfl_sync(0xffffffffu, ys[k], t) - hc;
+          if (nb < 0) continue;  // uniform over the warp
+          const float w0 = a0 == 0 ? wx[0] : (a0 == 1 ? wx[1] : (a0 == 2 ? wx[2] : wx[3]));
+          const float w1 = a1 == 0 ? wy4[0] : (a1 == 1 ? wy4[1] : (a1 == 2 ? wy4[2] : wy4[3]));
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int a2 = a2b + 2 * h;
+            const float w2 = a2 == 0 ? wz4[0] : (a2 == 1 ? wz4[1] : (a2 == 2 ? wz4[2] : wz4[3]));
+            const float wt = (w1 * w2) * w0;  // the product order of the loop below
+            const int node = nb + a0 + R * (a1 + R * a2);
+            atomicAdd(&acc[node], wt);
+#pragma unroll
+            for (int k = 0; k < 3; k++) atomicAdd(&acc[(k + 1) * RD + node], wt * qc[k]);
+          }
+        }
+      }
+    } else {
     // each thread walks its own contiguous stretch of the chunk, so the lanes
     // of a warp sit far apart in the (spatially ordered) chunk and their
     // shared-memory atomics rarely meet on one node
@@ -462,6 +530,7 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
             for (int k = 0; k < D; k++) atomicAdd(&acc[(k + 1) * RD + node], wt * (ys[k] - hc));
           }
         }
+    }
     }
     __syncthreads();
     // flush the touched region of this tile into V
