@@ -49,8 +49,7 @@ struct SgtState {
   float scale;       // float(N - 3): scaled coords lie in [0, N-3)
   float h_eff;       // grid spacing in embedding units
   int N;             // grid points per axis (n1 + 2)
-  int M;             // FFT length per axis (power of two >= 2N-1)
-  int logM;
+  int M;             // FFT length per axis (2^k or 3 * 2^k, >= 2N-1)
   int T;             // tile edge in cells
   int tiles_dim;     // tiles per axis
   int ntiles;

@@ -4,18 +4,19 @@
 // The reference computes it as 2^d half-shifted size-N cyclic convolutions
 // with cuFFT (CU/non_periodic_convF.cu:14-517, HYB/non_periodic_conv.cpp);
 // the sum of those terms is exactly the aperiodic convolution.  Here the
-// same convolution is one cyclic convolution of length M = 2^k >= 2N-1 per
-// axis: output nodes x < N only meet kernel offsets |x - x'| <= N-1 <= M/2,
-// so K_c[r] = K(min(r, M-r)) reproduces it.  Two real charge channels ride in
+// same convolution is one cyclic convolution of length M >= 2N-1 per axis
+// (the smallest M = 2^k or 3 * 2^k): output nodes x < N only meet kernel
+// offsets |x - x'| <= N-1 <= M/2, so K_c[r] = K(min(r, M-r)) reproduces it.  Two real charge channels ride in
 // one complex plane (K_c is real and even, so its transform is real and the
 // channels separate after the inverse).
 //
 // FFTs are register-resident: one warp owns one line of M <= 1024 points, a
-// lane holds the E = M/32 points lane + 32 e; butterflies with span >= 32
-// stay inside a lane, shorter spans use warp shuffles.  Forward transforms
-// are decimation in frequency (natural order in, bit-reversed out) and
-// inverse transforms decimation in time (bit-reversed in, natural out), so
-// spectra stay bit-reversed in memory and no permutation pass exists.  Rows
+// lane holds the E = M/32 points lane + 32 e; butterflies whose span holds
+// whole lanes (and the radix-3 stage of M = 3 * 2^k) stay inside a lane,
+// shorter spans use warp shuffles.  Forward transforms are decimation in
+// frequency (natural order in, digit-reversed out) and inverse transforms
+// decimation in time (digit-reversed in, natural out), so spectra stay in
+// that order in memory and no permutation pass exists.  Rows
 // are read and written directly (coalesced); columns go through a shared
 // memory transpose of 8 adjacent columns so every global access is a 64-byte
 // segment.  Planes of zero charge (index >= N) are never stored or read.
@@ -26,6 +27,7 @@
 
 #define SGT_FFT_COLS 8  // columns per CTA in column passes (one per warp)
 #define SGT_FFT_PAD 1   // float2 padding per staged column
+#define SGT_FFT_MAXM 1024  // longest FFT: twiddle tables hold M entries
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -36,74 +38,123 @@ __device__ __forceinline__ float2 shfl_x2(float2 v, int m) {
   return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }
 
-// tw[j] = exp(-2 pi i j / M), j < M/2 (accurate sincospi)
+// tw[j] = exp(-2 pi i j / M), j < M (accurate sincospi)
 __device__ __forceinline__ void fft_twiddles(float2 *tw, int M) {
-  for (int j = threadIdx.x; j < (M >> 1); j += blockDim.x) {
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
     float s, c;
     sincospif(2.0f * (float)j / (float)M, &s, &c);
     tw[j] = make_float2(c, -s);
   }
 }
 
-// forward DIF: natural order in, bit-reversed out (position i holds X[brev i])
-template <int LOGM>
+// FFT lengths: 2^k or 3 * 2^k, 32 <= M <= 1024.  A lane holds E = M/32
+// points, lane + 32 e.  Forward (DIF): radix-2 stages whose span holds whole
+// lanes (span >= 32, or >= 96 when M has the factor 3) run inside the lane;
+// for M = 3 * 2^k a radix-3 stage at span 32 follows, also inside the lane
+// (elements e, e+1, e+2 of a 96-point block, then twiddles W_96^(lane k));
+// the last five radix-2 stages (spans 16 .. 1) exchange between lanes by
+// shuffles.  The output order is the digit reversal these stages imply; the
+// inverse (DIT, conjugate twiddles, unscaled) applies the same stages in
+// reverse order and takes that order back to natural order, so spectra are
+// only ever multiplied pointwise in the permuted order.
+template <int M>
+struct FftLen {
+  static constexpr bool R3 = (M % 3) == 0;
+  static constexpr int E = M / 32;
+  static constexpr int LANE_MIN = R3 ? 96 : 32;  // smallest in-lane radix-2 span
+};
+
+template <int M>
 __device__ __forceinline__ void wfft_dif(float2 *v, const float2 *__restrict__ tw) {
-  constexpr int E = (1 << LOGM) / 32;
+  constexpr int E = FftLen<M>::E;
   const int lane = threadIdx.x & 31;
+  // in-lane radix-2 stages
 #pragma unroll
-  for (int s = LOGM - 1; s >= 0; s--) {
-    const int hs = 1 << s, sh = LOGM - 1 - s;
-    if (hs >= 32) {
-      const int he = hs >> 5;
+  for (int hs = M / 2; hs >= FftLen<M>::LANE_MIN; hs /= 2) {
+    if ((hs & 31) != 0) continue;
+    const int he = hs / 32, stride = M / (2 * hs);
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        if ((e & he) == 0) {
-          const float2 w = tw[((lane + 32 * e) & (hs - 1)) << sh];
-          const float2 u = v[e], t = v[e + he];
-          v[e] = cadd(u, t);
-          v[e + he] = cmul(csub(u, t), w);
-        }
+    for (int e = 0; e < E; e++) {
+      if ((e / he) % 2 == 0) {
+        const float2 w = tw[((lane + 32 * e) % hs) * stride];
+        const float2 u = v[e], t = v[e + he];
+        v[e] = cadd(u, t);
+        v[e + he] = cmul(csub(u, t), w);
       }
-    } else {
-      const bool upper = (lane & hs) != 0;
-      const float2 w = tw[(lane & (hs - 1)) << sh];
+    }
+  }
+  if constexpr (FftLen<M>::R3) {
+    // radix 3 over elements e, e+1, e+2 (positions i, i+32, i+64 of a
+    // 96-point block), then twiddles W_96^(lane k)
+    const float s3 = 0.8660254037844386f;  // sqrt(3)/2
+    const float2 w1 = tw[lane * (M / 96)], w2 = tw[2 * lane * (M / 96)];
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        const float2 x = v[e], y = shfl_x2(x, hs);
-        v[e] = upper ? cmul(csub(y, x), w) : cadd(x, y);
-      }
+    for (int e = 0; e < E; e += 3) {
+      const float2 a = v[e], b = v[e + 1], c = v[e + 2];
+      const float2 sm = cadd(b, c), df = csub(b, c);
+      const float2 t = make_float2(a.x - 0.5f * sm.x, a.y - 0.5f * sm.y);
+      const float2 u = make_float2(s3 * df.y, -s3 * df.x);  // -i sqrt(3)/2 (b - c)
+      v[e] = cadd(a, sm);
+      v[e + 1] = cmul(cadd(t, u), w1);
+      v[e + 2] = cmul(csub(t, u), w2);
+    }
+  }
+  // shuffle radix-2 stages, spans 16 .. 1
+#pragma unroll
+  for (int hs = 16; hs >= 1; hs /= 2) {
+    const bool upper = (lane & hs) != 0;
+    const float2 w = tw[(lane & (hs - 1)) * (M / (2 * hs))];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const float2 x = v[e], y = shfl_x2(x, hs);
+      v[e] = upper ? cmul(csub(y, x), w) : cadd(x, y);
     }
   }
 }
 
-// inverse DIT (conjugate twiddles, unscaled): bit-reversed in, natural out
-template <int LOGM>
+template <int M>
 __device__ __forceinline__ void wfft_dit_inv(float2 *v, const float2 *__restrict__ tw) {
-  constexpr int E = (1 << LOGM) / 32;
+  constexpr int E = FftLen<M>::E;
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int s = 0; s < LOGM; s++) {
-    const int hs = 1 << s, sh = LOGM - 1 - s;
-    if (hs >= 32) {
-      const int he = hs >> 5;
+  for (int hs = 1; hs <= 16; hs *= 2) {
+    const bool upper = (lane & hs) != 0;
+    float2 w = tw[(lane & (hs - 1)) * (M / (2 * hs))];
+    w.y = -w.y;
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        if ((e & he) == 0) {
-          float2 w = tw[((lane + 32 * e) & (hs - 1)) << sh];
-          w.y = -w.y;
-          const float2 u = v[e], t = cmul(v[e + he], w);
-          v[e] = cadd(u, t);
-          v[e + he] = csub(u, t);
-        }
-      }
-    } else {
-      const bool upper = (lane & hs) != 0;
-      float2 w = tw[(lane & (hs - 1)) << sh];
-      w.y = -w.y;
+    for (int e = 0; e < E; e++) {
+      const float2 x = v[e], y = shfl_x2(x, hs);
+      v[e] = upper ? csub(y, cmul(x, w)) : cadd(x, cmul(y, w));
+    }
+  }
+  if constexpr (FftLen<M>::R3) {
+    const float s3 = 0.8660254037844386f;
+    float2 w1 = tw[lane * (M / 96)], w2 = tw[2 * lane * (M / 96)];
+    w1.y = -w1.y;
+    w2.y = -w2.y;
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        const float2 x = v[e], y = shfl_x2(x, hs);
-        v[e] = upper ? csub(y, cmul(x, w)) : cadd(x, cmul(y, w));
+    for (int e = 0; e < E; e += 3) {
+      const float2 a = v[e], b = cmul(v[e + 1], w1), c = cmul(v[e + 2], w2);
+      const float2 sm = cadd(b, c), df = csub(b, c);
+      const float2 t = make_float2(a.x - 0.5f * sm.x, a.y - 0.5f * sm.y);
+      const float2 u = make_float2(-s3 * df.y, s3 * df.x);  // +i sqrt(3)/2 (b - c)
+      v[e] = cadd(a, sm);
+      v[e + 1] = cadd(t, u);
+      v[e + 2] = csub(t, u);
+    }
+  }
+#pragma unroll
+  for (int hs = FftLen<M>::LANE_MIN; hs <= M / 2; hs *= 2) {
+    if ((hs & 31) != 0) continue;
+    const int he = hs / 32, stride = M / (2 * hs);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if ((e / he) % 2 == 0) {
+        float2 w = tw[((lane + 32 * e) % hs) * stride];
+        w.y = -w.y;
+        const float2 u = v[e], t = cmul(v[e + he], w);
+        v[e] = cadd(u, t);
+        v[e + he] = csub(u, t);
       }
     }
   }
@@ -122,23 +173,28 @@ __device__ __forceinline__ float2 node_plane(const typename Node<D>::T &v, int p
   else return p == 0 ? make_float2(v.x, v.y) : make_float2(v.z, D == 3 ? v.w : 0.f);
 }
 
-#define SGT_FFT_DISPATCH(LOGM_EXPR, CALL)         \
-  switch (LOGM_EXPR) {                            \
-    case 5: CALL(5); break;                       \
-    case 6: CALL(6); break;                       \
-    case 7: CALL(7); break;                       \
-    case 8: CALL(8); break;                       \
-    case 9: CALL(9); break;                       \
-    default: CALL(10); break;                     \
+// the FFT lengths the grid decision picks (sgt_fft_length)
+#define SGT_FFT_DISPATCH(M_EXPR, CALL)            \
+  switch (M_EXPR) {                               \
+    case 32: CALL(32); break;                     \
+    case 64: CALL(64); break;                     \
+    case 96: CALL(96); break;                     \
+    case 128: CALL(128); break;                   \
+    case 192: CALL(192); break;                   \
+    case 256: CALL(256); break;                   \
+    case 384: CALL(384); break;                   \
+    case 512: CALL(512); break;                   \
+    case 768: CALL(768); break;                   \
+    default: CALL(1024); break;                   \
   }
 
 // ---------------------------------------------------------------------------
 // d = 1: the whole convolution in one warp
 // ---------------------------------------------------------------------------
-template <int LOGM>
+template <int M>
 __device__ void conv1d_body(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi,
                             const float2 *tw) {
-  constexpr int M = 1 << LOGM, E = M / 32;
+  constexpr int E = M / 32;
   const int N = st->N, lane = threadIdx.x & 31;
   const float hsq = st->h_eff * st->h_eff;
   float2 k[E], v[E];
@@ -148,11 +204,11 @@ __device__ void conv1d_body(const SgtState *st, const float2 *__restrict__ V, fl
     k[e] = make_float2(kern_val(hsq, M, x, 0, 0), 0.f);
     v[e] = x < N ? V[x] : make_float2(0.f, 0.f);
   }
-  wfft_dif<LOGM>(k, tw);
-  wfft_dif<LOGM>(v, tw);
+  wfft_dif<M>(k, tw);
+  wfft_dif<M>(v, tw);
 #pragma unroll
   for (int e = 0; e < E; e++) v[e] = make_float2(v[e].x * k[e].x, v[e].y * k[e].x);
-  wfft_dit_inv<LOGM>(v, tw);
+  wfft_dit_inv<M>(v, tw);
   const float inv = 1.0f / (float)M;
 #pragma unroll
   for (int e = 0; e < E; e++) {
@@ -163,12 +219,12 @@ __device__ void conv1d_body(const SgtState *st, const float2 *__restrict__ V, fl
 
 __global__ void __launch_bounds__(SGT_THREADS)
 k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi) {
-  __shared__ float2 tw[512];
+  __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
   if (threadIdx.x >= 32) return;
 #define C1(L) conv1d_body<L>(st, V, Phi, tw)
-  SGT_FFT_DISPATCH(st->logM, C1)
+  SGT_FFT_DISPATCH(st->M, C1)
 #undef C1
 }
 
@@ -177,10 +233,10 @@ k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ 
 // of the kernel plane (all rows), forward FFT along x.
 // W plane p at W + p * M^d; the kernel plane is p = 2.
 // ---------------------------------------------------------------------------
-template <int D, int LOGM>
+template <int D, int M>
 __device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *__restrict__ V,
                                 float2 *__restrict__ W, const float2 *tw) {
-  constexpr int M = 1 << LOGM, E = M / 32;
+  constexpr int E = M / 32;
   const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float hsq = st->h_eff * st->h_eff;
   const long plane = D == 2 ? (long)M * M : (long)M * M * M;
@@ -209,7 +265,7 @@ __device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *_
 #pragma unroll
       for (int e = 0; e < E; e++) v[e] = make_float2(kern_val(hsq, M, lane + 32 * e, y, z), 0.f);
     }
-    wfft_dif<LOGM>(v, tw);
+    wfft_dif<M>(v, tw);
     float2 *row = W + p * plane + (long)M * y + (D == 3 ? (long)M * M * z : 0);
 #pragma unroll
     for (int e = 0; e < E; e++) row[lane + 32 * e] = v[e];
@@ -219,11 +275,11 @@ __device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *_
 template <int D>
 __global__ void __launch_bounds__(SGT_THREADS)
 k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
-  __shared__ float2 tw[512];
+  __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
 #define CB(L) build_rows_body<D, L>(st, V, W, tw)
-  SGT_FFT_DISPATCH(st->logM, CB)
+  SGT_FFT_DISPATCH(st->M, CB)
 #undef CB
 }
 
@@ -238,29 +294,29 @@ k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V, flo
 #define MODE_MID_FWD 1
 #define MODE_MID_INV 2
 
-template <int LOGM>
+template <int M>
 __device__ __forceinline__ void stage_load(float2 *stg, const float2 *__restrict__ src, long stride,
                                            int lim) {
-  constexpr int M = 1 << LOGM, LS = M + SGT_FFT_PAD;
+  constexpr int LS = M + SGT_FFT_PAD;
   for (int idx = threadIdx.x; idx < SGT_FFT_COLS * M; idx += blockDim.x) {
     const int t = idx / SGT_FFT_COLS, c = idx % SGT_FFT_COLS;
     stg[c * LS + t] = t < lim ? src[(long)t * stride + c] : make_float2(0.f, 0.f);
   }
 }
-template <int LOGM>
+template <int M>
 __device__ __forceinline__ void stage_store(const float2 *stg, float2 *__restrict__ dst, long stride,
                                             int lim) {
-  constexpr int M = 1 << LOGM, LS = M + SGT_FFT_PAD;
+  constexpr int LS = M + SGT_FFT_PAD;
   for (int idx = threadIdx.x; idx < SGT_FFT_COLS * lim; idx += blockDim.x) {
     const int t = idx / SGT_FFT_COLS, c = idx % SGT_FFT_COLS;
     dst[(long)t * stride + c] = stg[c * LS + t];
   }
 }
 
-template <int D, int MODE, int LOGM>
+template <int D, int MODE, int M>
 __device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const float2 *tw,
                           float2 *stg, float *kre) {
-  constexpr int M = 1 << LOGM, E = M / 32, LS = M + SGT_FFT_PAD;
+  constexpr int E = M / 32, LS = M + SGT_FFT_PAD;
   const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long plane = D == 2 ? (long)M * M : (long)M * M * M;
   const int ncb = M / SGT_FFT_COLS;
@@ -278,31 +334,31 @@ __device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const floa
     if (MODE == MODE_LAST) {
       const long off = (long)cb * SGT_FFT_COLS + (D == 3 ? (long)M * rest : 0);
       // kernel spectrum of the 8 columns, real part kept
-      stage_load<LOGM>(stg, W + 2 * plane + off, stride, M);
+      stage_load<M>(stg, W + 2 * plane + off, stride, M);
       __syncthreads();
 #pragma unroll
       for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
-      wfft_dif<LOGM>(v, tw);
+      wfft_dif<M>(v, tw);
 #pragma unroll
       for (int e = 0; e < E; e++) kre[warp * M + lane + 32 * e] = v[e].x;
       for (int p = 0; p < 2; p++) {
         float2 *base = W + p * plane + off;
         __syncthreads();
-        stage_load<LOGM>(stg, base, stride, N);
+        stage_load<M>(stg, base, stride, N);
         __syncthreads();
 #pragma unroll
         for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
-        wfft_dif<LOGM>(v, tw);
+        wfft_dif<M>(v, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) {
           const float kr = kre[warp * M + lane + 32 * e];
           v[e] = make_float2(v[e].x * kr, v[e].y * kr);
         }
-        wfft_dit_inv<LOGM>(v, tw);
+        wfft_dit_inv<M>(v, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) stg[warp * LS + lane + 32 * e] = v[e];
         __syncthreads();
-        stage_store<LOGM>(stg, base, stride, N);
+        stage_store<M>(stg, base, stride, N);
       }
     } else {
       int p, z;
@@ -315,25 +371,25 @@ __device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const floa
       }
       float2 *base = W + p * plane + (long)M * M * z + (long)cb * SGT_FFT_COLS;
       if (MODE == MODE_MID_FWD) {
-        stage_load<LOGM>(stg, base, M, p == 2 ? M : N);
+        stage_load<M>(stg, base, M, p == 2 ? M : N);
         __syncthreads();
 #pragma unroll
         for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
-        wfft_dif<LOGM>(v, tw);
+        wfft_dif<M>(v, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) stg[warp * LS + lane + 32 * e] = v[e];
         __syncthreads();
-        stage_store<LOGM>(stg, base, M, M);
+        stage_store<M>(stg, base, M, M);
       } else {
-        stage_load<LOGM>(stg, base, M, M);
+        stage_load<M>(stg, base, M, M);
         __syncthreads();
 #pragma unroll
         for (int e = 0; e < E; e++) v[e] = stg[warp * LS + lane + 32 * e];
-        wfft_dit_inv<LOGM>(v, tw);
+        wfft_dit_inv<M>(v, tw);
 #pragma unroll
         for (int e = 0; e < E; e++) stg[warp * LS + lane + 32 * e] = v[e];
         __syncthreads();
-        stage_store<LOGM>(stg, base, M, N);
+        stage_store<M>(stg, base, M, N);
       }
     }
   }
@@ -344,12 +400,12 @@ __global__ void __launch_bounds__(SGT_THREADS)
 k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
   extern __shared__ float2 sm[];
   float2 *tw = sm;
-  float2 *stg = sm + 512;
+  float2 *stg = sm + SGT_FFT_MAXM;
   float *kre = reinterpret_cast<float *>(stg + SGT_FFT_COLS * (st->M + SGT_FFT_PAD));
   fft_twiddles(tw, st->M);
   __syncthreads();
 #define CC(L) cols_body<D, MODE, L>(st, W, tw, stg, kre)
-  SGT_FFT_DISPATCH(st->logM, CC)
+  SGT_FFT_DISPATCH(st->M, CC)
 #undef CC
 }
 
@@ -357,10 +413,10 @@ k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
 // final pass: inverse FFT along x of rows y (, z) < N, scale by 1/M^d, write
 // the potential grid (channels packed per node: plane 0 -> .xy, 1 -> .zw).
 // ---------------------------------------------------------------------------
-template <int D, int LOGM>
+template <int D, int M>
 __device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W,
                                 float2 *__restrict__ Phi2, const float2 *tw) {
-  constexpr int M = 1 << LOGM, E = M / 32;
+  constexpr int E = M / 32;
   const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long plane = D == 2 ? (long)M * M : (long)M * M * M;
   const long lines = 2L * N * (D == 3 ? N : 1);
@@ -376,7 +432,7 @@ __device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W
     float2 v[E];
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = row[lane + 32 * e];
-    wfft_dit_inv<LOGM>(v, tw);
+    wfft_dit_inv<M>(v, tw);
     const long g0 = (long)N * y + (D == 3 ? (long)N * N * z : 0);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -389,16 +445,16 @@ __device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W
 template <int D>
 __global__ void __launch_bounds__(SGT_THREADS)
 k_fft_final_x(const SgtState *st, const float2 *__restrict__ W, typename Node<D>::T *__restrict__ Phi) {
-  __shared__ float2 tw[512];
+  __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
 #define CF(L) final_rows_body<D, L>(st, W, reinterpret_cast<float2 *>(Phi), tw)
-  SGT_FFT_DISPATCH(st->logM, CF)
+  SGT_FFT_DISPATCH(st->M, CF)
 #undef CF
 }
 
 // shared memory of a column pass for FFT length Mmax
 __host__ __device__ inline size_t fft_cols_smem(int Mmax) {
-  return sizeof(float2) * (512 + (size_t)SGT_FFT_COLS * (Mmax + SGT_FFT_PAD)) +
+  return sizeof(float2) * (SGT_FFT_MAXM + (size_t)SGT_FFT_COLS * (Mmax + SGT_FFT_PAD)) +
          sizeof(float) * (size_t)SGT_FFT_COLS * Mmax;
 }

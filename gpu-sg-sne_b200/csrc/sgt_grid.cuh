@@ -19,6 +19,19 @@
 
 #define SGT_HIST_MAX 4096  // tiles held in shared memory by the binning kernels
 
+// Smallest FFT length >= need among 32, 64, 96, 128, 192, ..., 768, 1024
+// (2^k and 3 * 2^k): the 3 * 2^k lengths cut the padding of grids just above
+// a power of two (N = 33..48 takes 96 points per axis instead of 128).
+__device__ __forceinline__ int sgt_fft_length(int need) {
+  int m = 32;
+  while (m < 1024) {
+    if (m >= need) return m;
+    if (m >= 64 && (m / 2) * 3 >= need) return (m / 2) * 3;
+    m <<= 1;
+  }
+  return 1024;
+}
+
 // ---------------------------------------------------------------------------
 // Grid decision from the stats of the coordinates that the next kernels bin.
 // minv/maxv are per-dim min/max of Ynext, sums its per-dim sums; the
@@ -54,8 +67,7 @@ __device__ void sgt_finalize_grid(SgtState *st, const SgtJobParams &jp,
     n1 = sgt_best_grid_size_dev(ng);
   }
   int N = n1 + 2;
-  int M = 1, logM = 0;
-  while (M < 2 * N - 1) { M <<= 1; logM++; }
+  int M = sgt_fft_length(2 * N - 1);
   if (M > jp.mmax) {  // keep the grid inside the allocated FFT workspace
     st->error |= SGT_EFLAG_GRID_CLAMP;
     st->grid_clamped = 1;
@@ -63,13 +75,11 @@ __device__ void sgt_finalize_grid(SgtState *st, const SgtJobParams &jp,
     while (i > 0 && 2 * c_grid_sizes[i] - 1 > jp.mmax) i--;
     N = c_grid_sizes[i];
     n1 = N - 2;
-    M = 1; logM = 0;
-    while (M < 2 * N - 1) { M <<= 1; logM++; }
+    M = sgt_fft_length(2 * N - 1);
   }
   st->maxy = maxy;
   st->N = N;
   st->M = M;
-  st->logM = logM;
   st->scale = (float)(unsigned)(N - 3);
   st->h_eff = __fdiv_rn(maxy, (float)(n1 - 1) - 1.1920928955078125e-7f);
   const int cells = n1 - 1;  // floor bins lie in [0, n1-2]

@@ -434,3 +434,27 @@ def test_symmetrize_device_rejects_bad_column(torch, ctx):
     with pytest.raises(S.SgtError) as e:
         ctx.symmetrize(2, 3, dev(torch, rp), dev(torch, col), dev(torch, val), 0.25, orp, oc, ov)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("ng", [40, 80])
+def test_mixed_radix_fft_lengths(torch, ctx, oracle, d, ng):
+    """Fixed grids whose FFT length has the factor 3: ng = 40 gives N = 42
+    (2N-1 = 83, M = 96) and ng = 80 gives N = 84 (M = 192).  The potential
+    grid against the oracle's G2G of the engine's own charge grid, and the
+    forces against the oracle at the same grid."""
+    import sgtsne_b200 as S
+    n = 6000
+    Y = coords("clusters", n, d, seed=60 + d)
+    h = {1: 0.5, 2: 0.7, 3: 1.2}[d]
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    Z, N, he = ctx.repulsive(n, d, h, ng, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    assert N == S.best_grid_size(ng) + 2
+    assert 2 * N - 1 in range(65, 97) if ng == 40 else 2 * N - 1 in range(129, 193)
+    V, Phi = ctx.last_grids(d, N)
+    Phio = oracle.g2g(V.astype(np.float64), float(he), 0)
+    assert rel(Phi, Phio) <= 1e-4
+    Fo, Zo, No, _ = oracle.repulsive_interp(Y.astype(np.float64), h, n1_force=N - 2)
+    assert No == N
+    assert rel(f.cpu().numpy().reshape(n, d), Fo) <= 3e-4
+    assert abs(Z - Zo) <= 5e-4 * abs(Zo)
