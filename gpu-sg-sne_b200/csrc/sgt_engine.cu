@@ -505,26 +505,28 @@ static sgt_status enqueue_repulsion(sgt_job *J, cudaStream_t s, cudaEvent_t *ev 
   return enqueue_repulsion_rest<D>(J, s, ev);
 }
 
-// F_attr of the centred Y in the job's format
+// F_attr in the job's format.  It depends on coordinate differences only,
+// so it reads Ynext (the coordinates before the binning pass subtracts
+// their mean) and need not wait for that pass.
 template <int D, int G>
 static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   const int n = J->n;
+  const VT *Yc = (const VT *)J->Ynext;
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)J->Y,
-                                                 (VT *)J->Fattr, n);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
-      k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals,
-                                                      (const VT *)J->Y, (VT *)J->Fattr);
+      k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals, Yc,
+                                                      (VT *)J->Fattr);
     } else {
       CK(cudaMemsetAsync(J->Fattr, 0, sizeof(float) * (size_t)n * J->S, s));
     }
     if (J->coo_n > 0)
       k_attr_coo<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(J->coo_n, J->coo_rows, J->coo_cols,
-                                                      J->coo_vals, (const VT *)J->Y, J->Fattr);
+                                                      J->coo_vals, Yc, J->Fattr);
   }
   CK(cudaGetLastError());
   return SGT_OK;
@@ -554,19 +556,20 @@ static sgt_status enqueue_combine(sgt_job *J, cudaStream_t s) {
   return SGT_OK;
 }
 
-// One iteration.  After the binning pass has written the centred Y, the
-// attractive SpMV (bound by L1 gather throughput) and the rest of the
-// repulsion chain (a series of latency-bound kernels) both read only Y:
-// the SpMV is forked onto the context's side stream and joined before the
-// combine, so in the captured graph the two run concurrently.
+// One iteration.  The attractive SpMV (bound by L1 gather throughput) reads
+// only Ynext and P; the repulsion chain (a series of latency-bound kernels,
+// starting with the binning pass that writes the centred Y) reads only
+// Ynext and its own buffers.  The SpMV is forked onto the context's side
+// stream and joined before the combine, so in the captured graph the two
+// run concurrently.
 template <int D>
 static sgt_status enqueue_iteration(sgt_job *J, cudaStream_t s) {
   sgt_ctx *ctx = J->ctx;
-  CKS(enqueue_bin_count<D>(J, s));
   CK(cudaEventRecord(J->ev_fork, s));
   CK(cudaStreamWaitEvent(ctx->side, J->ev_fork, 0));
   CKS(dispatch_attractive<D>(J, ctx->side));
   CK(cudaEventRecord(J->ev_join, ctx->side));
+  CKS(enqueue_bin_count<D>(J, s));
   CKS(enqueue_repulsion_rest<D>(J, s));
   CK(cudaStreamWaitEvent(s, J->ev_join, 0));
   return enqueue_combine<D>(J, s);

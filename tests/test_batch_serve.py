@@ -6,10 +6,13 @@ to run, and the t-SNE iteration amplifies such last-bit differences (a
 difference in maxy that flips the grid-size decision moves the forces by the
 interpolation error, ~1e-3): two plain runs of one job from the same Y0
 differ by rel-L2 ~1e-7 after 2 iterations, up to ~1e-4 after 5 and up to
-~1e-2 after 40.  So:
+~1e-2 after 40.  KL is compared once the early exaggeration has ended and
+the embedding has relaxed (exaggeration for 100 iterations, KL after 300):
+there, four plain runs of each job below spread by at most 0.4 % in KL,
+where during the exaggeration they spread by up to 1.1 %.  So:
 
   after 2 iterations     Y alone vs in the mix        rel-L2 <= 1e-5
-  after 200 iterations   KL alone vs in the mix       within 1 %
+  after 300 iterations   KL alone vs in the mix       within 1 %
 """
 import numpy as np
 import pytest
@@ -20,7 +23,8 @@ pytestmark = pytest.mark.gpu
 
 TOL_Y = 1e-5     # Y after SHORT iterations
 SHORT = 2
-LONG = 200
+LONG = 300
+EARLY = 100      # iterations of early exaggeration
 TOL_KL = 0.01    # relative KL after LONG iterations
 
 
@@ -49,7 +53,7 @@ def problems():
 
 
 def params(S, d, iters):
-    return S.default_params(d=d, format=S.FORMAT_CSR, max_iter=iters, early_iter=250,
+    return S.default_params(d=d, format=S.FORMAT_CSR, max_iter=iters, early_iter=EARLY,
                             h=0.7 if d == 2 else 1.2)
 
 
