@@ -142,10 +142,17 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def build_knn(n, seed, device):
+def build_knn(n, seed, device, ctx=None):
+    """The 1.3M-point configuration's points and their exact 30 nearest
+    neighbours: through the engine (sgt_knn) when a context is given, else
+    with torch matrix products (the reference arm on a host without the
+    engine's device)."""
     from sgtsne_b200 import workloads as W
     X, _ = W.gmm_zipf(n, dim=50, ncomp=40, zipf_a=1.1, centre_var=25.0, seed=seed)
-    idx, d2 = W.knn_torch(X, 30, device=device, block=1024)
+    if ctx is not None:
+        idx, d2 = W.knn_engine(ctx, X, 30, device)
+    else:
+        idx, d2 = W.knn_torch(X, 30, device=device, block=1024)
     if str(device).startswith("cuda"):
         import torch
         torch.cuda.synchronize()
@@ -215,7 +222,7 @@ def build_problem(args, dev, ctx):
 
     import sgtsne_b200 as S
     n = args.n
-    X, idx, d2 = build_knn(n, args.seed, dev)
+    X, idx, d2 = build_knn(n, args.seed, dev, ctx)
     k = idx.shape[1]
     rp_knn = torch.arange(0, (n + 1) * k, k, dtype=torch.int32, device=dev)
     vals = d2.reshape(-1).contiguous().clone()
@@ -475,7 +482,11 @@ def run_reference(args, rank, world, local, dist):
     from oracle import oracle as O
     dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
     n = args.n
-    X, idx, d2 = build_knn(n, args.seed, dev)
+    ctx = None
+    if torch.cuda.is_available():  # the same P as the engine's arm (setup only)
+        import sgtsne_b200 as S
+        ctx = S.Context(local)
+    X, idx, d2 = build_knn(n, args.seed, dev, ctx)
     k = idx.shape[1]
     rp = (np.arange(n + 1, dtype=np.int64) * k).astype(np.int32)
     col = idx.reshape(-1).cpu().numpy().astype(np.int32)

@@ -8,14 +8,19 @@
 //                     [-G fixed|h] [-k kNN-file-is-P: 0|1] FILE
 // FILE holds either a sparse stochastic matrix in Matrix Market coordinate
 // format (1-based "row col value", as buildPFromMTX, CU/utils.cu:335-409) or
-// dense points ("n d" then n*d values, as readXfromMTX, CU/utils.cu:216-256).
-// Dense point input (the kNN stage of the reference) is not part of this
-// build; it reports so and exits.
+// dense points ("n d" then n*d values, as readXfromMTX, CU/utils.cu:216-256;
+// -n takes the first n points).  Dense input goes through the stages of the
+// reference's demo_perplexity.cu:111-158 on the device: exact kNN with
+// ceil(3u) neighbours (sgt_knn, where the reference calls FLANN), distances
+// divided by their maximum, perplexity equalisation to u (sgt_perplexity),
+// then sgt_embed.
 // Outputs: sgtsneEmbedding.txt (one point per line) and timeInfo.txt.
 #include "sgtsne_b200.h"
 
+#include <cuda_runtime.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -67,6 +72,70 @@ static bool read_mtx(const std::string &fn, int &n, std::vector<int> &rp, std::v
     fill[cc]++;
   }
   return true;
+}
+
+static bool read_dense(const std::string &fn, int limit, int &n, int &dim,
+                       std::vector<float> &X) {
+  std::ifstream fin(fn);
+  if (!fin) return false;
+  long nn, dd;
+  if (!(fin >> nn >> dd) || nn < 2 || dd < 1) return false;
+  if (limit > 0 && limit < nn) nn = limit;
+  n = (int)nn;
+  dim = (int)dd;
+  X.resize((size_t)n * dim);
+  for (size_t l = 0; l < X.size(); l++)
+    if (!(fin >> X[l])) return false;
+  return true;
+}
+
+// kNN -> max-normalised distances -> perplexity rows, as host CSR with
+// ceil(3u) entries per row (CU/testing_modules/demo_perplexity.cu:98-158)
+static sgt_status dense_to_p(sgt_ctx *ctx, int n, int dim, const std::vector<float> &X, float u,
+                             std::vector<int> &rp, std::vector<int> &col,
+                             std::vector<float> &val) {
+  const int nn = (int)std::ceil(u * 3);
+  if (nn >= n) return SGT_ERR_INVALID_ARG;
+  float *dX = nullptr, *dD = nullptr, *dP = nullptr;
+  int *dI = nullptr;
+  const size_t m = (size_t)n * nn;
+  sgt_status st = SGT_OK;
+  if (cudaMalloc(&dX, sizeof(float) * X.size()) != cudaSuccess ||
+      cudaMalloc(&dD, sizeof(float) * m) != cudaSuccess ||
+      cudaMalloc(&dP, sizeof(float) * m) != cudaSuccess ||
+      cudaMalloc(&dI, sizeof(int) * m) != cudaSuccess)
+    st = SGT_ERR_NO_MEMORY;
+  if (st == SGT_OK &&
+      cudaMemcpy(dX, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    st = SGT_ERR_CUDA;
+  if (st == SGT_OK) st = sgt_knn(ctx, n, dim, dX, nn, dI, dD);
+  std::vector<float> D(m);
+  if (st == SGT_OK &&
+      cudaMemcpy(D.data(), dD, sizeof(float) * m, cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = SGT_ERR_CUDA;
+  if (st == SGT_OK) {
+    float mx = 0.f;
+    for (float v : D) mx = std::max(mx, v);
+    if (mx > 0)
+      for (float &v : D) v /= mx;
+    if (cudaMemcpy(dD, D.data(), sizeof(float) * m, cudaMemcpyHostToDevice) != cudaSuccess)
+      st = SGT_ERR_CUDA;
+  }
+  if (st == SGT_OK) st = sgt_perplexity(ctx, n, nn, dD, u, dP, nullptr);
+  if (st == SGT_OK) {
+    col.resize(m);
+    val.resize(m);
+    rp.resize((size_t)n + 1);
+    for (int i = 0; i <= n; i++) rp[i] = i * nn;
+    if (cudaMemcpy(col.data(), dI, sizeof(int) * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(val.data(), dP, sizeof(float) * m, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = SGT_ERR_CUDA;
+  }
+  cudaFree(dX);
+  cudaFree(dD);
+  cudaFree(dP);
+  cudaFree(dI);
+  return st;
 }
 
 int main(int argc, char **argv) {
@@ -139,10 +208,21 @@ int main(int argc, char **argv) {
       return 1;
     }
   } else {
-    std::cerr << "dense point input needs the kNN stage, which this build does not ship;"
-                 " pass a sparse stochastic matrix (Matrix Market)" << std::endl;
-    sgt_destroy(ctx);
-    return 1;
+    int dim = 0;
+    std::vector<float> X;
+    if (!read_dense(filename, p.n, n, dim, X)) {
+      std::cerr << "cannot parse points " << filename << std::endl;
+      sgt_destroy(ctx);
+      return 1;
+    }
+    std::cout << "Number of points " << n << " dimensions " << dim << std::endl;
+    st = dense_to_p(ctx, n, dim, X, u, rp, col, val);
+    if (st != SGT_OK) {
+      std::cerr << "kNN / perplexity: " << sgt_status_string(st) << ": " << sgt_last_error(ctx)
+                << std::endl;
+      sgt_destroy(ctx);
+      return 2;
+    }
   }
   p.n = n;
   std::vector<float> y((size_t)n * (p.d > 0 ? p.d : 2));

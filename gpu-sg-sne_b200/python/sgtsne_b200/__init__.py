@@ -115,6 +115,7 @@ SIGNATURES = {
     "sgt_csr_to_hybrid": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_symmetrize": (_i, [_i, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_symmetrize_device": (_i, [_vp, _i, _l, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
+    "sgt_knn": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp]),
 }
 
 _LIB = None
@@ -236,6 +237,12 @@ class Context:
     def perplexity(self, n, k, dist, perp, p, beta=None):
         self.check(self.lib.sgt_perplexity(self.h, n, k, _ptr(dist), float(perp), _ptr(p),
                                            _ptr(beta)), "perplexity")
+
+    def knn(self, n, dim, X, k, idx, d2):
+        """Exact kNN (squared distances, self excluded) of device X (n*dim)
+        into device idx/d2 (n*k)."""
+        self.check(self.lib.sgt_knn(self.h, int(n), int(dim), _ptr(X), int(k), _ptr(idx),
+                                    _ptr(d2)), "knn")
 
     def symmetrize(self, n, nnz, rowptr, col, val, scale, out_rowptr, out_col, out_val):
         """(P + P^T) * scale on the device; out_col/out_val hold 2 nnz.

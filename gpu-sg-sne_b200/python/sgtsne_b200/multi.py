@@ -3,9 +3,9 @@ one CUDA graph) and the served workload (an open-loop request stream through
 the continuous-batching server), each beside its plain form (the same jobs
 run one after another through sgt_job_run).
 
-Used by bench.py.  P of every instance is built on the device (exact kNN
-with fp32 matrix products, lambda bisection and symmetrisation through the
-engine), as for the single-embedding benchmark.
+Used by bench.py.  P of every instance is built on the device through the
+engine (exact kNN, lambda bisection, symmetrisation), as for the
+single-embedding benchmark.
 """
 from __future__ import annotations
 
@@ -47,7 +47,7 @@ def batched_instances(ctx, count, seed, dev, n_lo=2000, n_hi=200000, k=30):
         ncomp = int(rng.integers(5, 31))
         d = 2 if i % 2 == 0 else 3
         X, _ = W.gmm_isotropic(n, dim, ncomp, 16.0, seed * 100003 + i, dtype=np.float32)
-        idx, d2 = W.knn_torch(X, k, device=dev, block=2048)
+        idx, d2 = W.knn_engine(ctx, X, k, dev)
         rp, col, val = _csr_from_knn(ctx, idx, d2, 1.0, dev)
         y0 = (np.random.default_rng(seed + 7 + i).standard_normal((n, d)) * 1e-2).astype(np.float32)
         out.append({"n": n, "d": d, "dim": dim, "rp": rp, "col": col, "val": val, "y0": y0})
@@ -66,7 +66,7 @@ def request_instances(ctx, count, seed, dev, n_lo=1000, n_hi=500000, k=30):
         lam = float(rng.choice([1.0, 10.0, 30.0]))
         iters = int(rng.integers(500, 1001))
         X, _ = W.gmm_zipf(n, 50, 40, 1.1, 25.0, seed * 100003 + i)
-        idx, d2 = W.knn_torch(X, k, device=dev, block=2048)
+        idx, d2 = W.knn_engine(ctx, X, k, dev)
         rp, col, val = _csr_from_knn(ctx, idx, d2, lam, dev)
         y0 = (np.random.default_rng(seed + 11 + i).standard_normal((n, d)) * 1e-2).astype(np.float32)
         out.append({"n": n, "d": d, "lambda": lam, "iters": iters, "rp": rp, "col": col,

@@ -90,6 +90,19 @@ def knn_numpy(X, k, block=2048):
     return idx, d2
 
 
+def knn_engine(ctx, X, k, device="cuda"):
+    """Exact kNN through the engine (sgt_knn): returns device tensors
+    idx (n, k) int32 and d2 (n, k) float32, rows sorted, self excluded."""
+    import torch
+    Xd = torch.as_tensor(np.ascontiguousarray(X, np.float32), device=device)
+    n, dim = Xd.shape
+    idx = torch.empty((n, k), dtype=torch.int32, device=device)
+    d2 = torch.empty((n, k), dtype=torch.float32, device=device)
+    torch.cuda.synchronize(device)  # X written by torch before the engine reads it
+    ctx.knn(n, dim, Xd, k, idx, d2)
+    return idx, d2
+
+
 def knn_torch(X, k, device="cuda", block=4096):
     """Exact kNN on the GPU with fp32 matrix products (setup only)."""
     import torch

@@ -331,6 +331,16 @@ sgt_status sgt_csr_to_hybrid(int n, const int *rowptr, const int *col,
                              unsigned *coo_cols, float *coo_vals,
                              long *coo_size);
 
+/* Exact k nearest neighbours of n points in dim dimensions: squared
+   Euclidean distances, the point itself excluded, each row sorted by
+   distance (ties by index).  X: device, row-major n*dim; idx, d2: device,
+   n*k.  1 <= k <= 128, k < n.  Replaces the kNN search of the reference's
+   command line tool (allKNNsearchflann, FLANN, approximate;
+   CU/testing_modules/demo_perplexity.cu:131) with an exact one; the result
+   feeds sgt_perplexity directly.  Synchronises the context's stream. */
+sgt_status sgt_knn(sgt_ctx *ctx, int n, int dim, const float *X, int k, int *idx,
+                   float *d2);
+
 /* The same on the device: device arrays, out_col/out_val sized 2*nnz (an
    upper bound), out_rowptr n+1; *out_nnz receives the count (synchronises
    the context's stream).  Bit-identical to sgt_symmetrize.  n <= 2^24,

@@ -15,6 +15,8 @@ Tolerances (FP32 engine vs FP64 oracle):
   lambda / perplexity values                              rel <= 1e-4
   iterations (same P, Y0): KL after the run               within 1 %
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -458,3 +460,100 @@ def test_mixed_radix_fft_lengths(torch, ctx, oracle, d, ng):
     assert No == N
     assert rel(f.cpu().numpy().reshape(n, d), Fo) <= 3e-4
     assert abs(Z - Zo) <= 5e-4 * abs(Zo)
+
+
+@pytest.mark.parametrize("n,dim,k", [(3000, 50, 30), (2500, 37, 90), (1800, 130, 15),
+                                     (700, 3, 1), (1500, 784, 128)])
+def test_knn_exact(torch, ctx, n, dim, k):
+    """sgt_knn against FP64 distances computed directly: the k-th distance of
+    every row within 1e-5, and the neighbour lists equal except where a
+    distance ties within FP32 rounding (at most 0.1 % of the entries)."""
+    import sgtsne_b200 as S
+    rng = np.random.default_rng(dim + k)
+    c = rng.standard_normal((8, dim)) * 4
+    X = (c[rng.integers(0, 8, n)] + rng.standard_normal((n, dim))).astype(np.float32)
+    idx = torch.empty(n * k, dtype=torch.int32, device="cuda")
+    d2 = torch.empty(n * k, dtype=torch.float32, device="cuda")
+    ctx.knn(n, dim, dev(torch, X), k, idx, d2)
+    I = idx.cpu().numpy().reshape(n, k)
+    Dg = d2.cpu().numpy().reshape(n, k).astype(np.float64)
+    X64 = X.astype(np.float64)
+    D = np.empty((n, n))
+    b = max(1, int(2e7 // (n * dim)))  # direct differences, b rows at a time
+    for s0 in range(0, n, b):
+        D[s0:s0 + b] = ((X64[s0:s0 + b, None, :] - X64[None, :, :]) ** 2).sum(-1)
+    np.fill_diagonal(D, np.inf)
+    order = np.argsort(D, axis=1, kind="stable")[:, :k]
+    Dref = np.take_along_axis(D, order, 1)
+    assert np.all(np.diff(Dg, axis=1) >= 0)                     # rows sorted
+    assert np.all(I != np.arange(n)[:, None])                   # self excluded
+    assert np.abs(Dg - Dref).max() <= 1e-5 * max(Dref.max(), 1.0)
+    same = np.mean([len(set(a) & set(b)) / k for a, b in zip(I, order)])
+    assert same >= 0.999
+    # the distances returned are those of the indices returned
+    Dchk = np.take_along_axis(D, I.astype(np.int64), 1)
+    assert np.abs(Dchk - Dg).max() <= 1e-5 * max(Dref.max(), 1.0)
+
+
+def test_knn_rejects_bad_k(torch, ctx):
+    import sgtsne_b200 as S
+    X = torch.zeros(10 * 3, dtype=torch.float32, device="cuda")
+    idx = torch.empty(10 * 200, dtype=torch.int32, device="cuda")
+    d2 = torch.empty(10 * 200, dtype=torch.float32, device="cuda")
+    for k in (10, 129):
+        with pytest.raises(S.SgtError) as e:
+            ctx.knn(10, 3, X, k, idx, d2)
+        assert e.value.status == 4
+
+
+def test_cli_dense_and_mtx(torch, ctx, oracle, tmp_path):
+    """sg_tsne_cuda on dense points (kNN, perplexity, embedding on the
+    device) and on a Matrix Market P: n finite, centred rows each, and the
+    dense run's KL within 2 % of the same pipeline driven from Python."""
+    import subprocess
+
+    import sgtsne_b200 as S
+    from sgtsne_b200 import workloads as W
+    exe = os.path.join(os.path.dirname(S.LIB_PATH), "..", "bin", "sg_tsne_cuda")
+    n, dim, u = 1500, 20, 10.0
+    X, _ = W.gmm_isotropic(n, dim, 6, 16.0, 3, dtype=np.float32)
+    with open(tmp_path / "pts.txt", "w") as f:
+        f.write(f"{n} {dim}\n")
+        np.savetxt(f, X, fmt="%.7g")
+    args = [exe, "-d", "2", "-m", "300", "-e", "100", "-u", str(u), "-t", "csr"]
+    r = subprocess.run(args + [str(tmp_path / "pts.txt")], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    Y = np.loadtxt(tmp_path / "sgtsneEmbedding.txt")
+    assert Y.shape == (n, 2) and np.isfinite(Y).all()
+    assert np.abs(Y.mean(0)).max() < 1e-3
+    # the same stages from Python: kNN, max-normalised distances, perplexity
+    nn = int(np.ceil(3 * u))
+    idx = torch.empty(n * nn, dtype=torch.int32, device="cuda")
+    d2 = torch.empty(n * nn, dtype=torch.float32, device="cuda")
+    ctx.knn(n, dim, dev(torch, X), nn, idx, d2)
+    D = d2 / d2.max()
+    Pk = torch.empty(n * nn, dtype=torch.float32, device="cuda")
+    ctx.perplexity(n, nn, D.contiguous(), u, Pk)
+    rp = (np.arange(n + 1) * nn).astype(np.int32)
+    col, val = idx.cpu().numpy(), Pk.cpu().numpy()
+    p = S.default_params(d=2, max_iter=300, early_iter=100, format=S.FORMAT_CSR)
+    Yp, _ = ctx.embed(rp, col, val, p)
+    srp, sc, sv = S.symmetrize(rp, col, val, 1.0 / (2 * n))
+
+    def kl(Yx):
+        _, Z, _, _ = oracle.repulsive_interp(Yx.astype(np.float64), 0.7)
+        return oracle.kl(srp, sc, sv.astype(np.float64), Yx.astype(np.float64), 1.0, Z)
+    assert abs(kl(Y) - kl(Yp)) <= 0.02 * kl(Yp)
+    # Matrix Market input: the symmetrised P written 1-based, column-major
+    rows = np.repeat(np.arange(n), np.diff(srp))
+    with open(tmp_path / "p.mtx", "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{n} {n} {len(sc)}\n")
+        for a, b, v in zip(sc, rows, sv):  # column-major: (row, col) of P^T
+            f.write(f"{b + 1} {a + 1} {v:.9g}\n")
+    r = subprocess.run([exe, "-d", "2", "-m", "100", "-t", "coo", str(tmp_path / "p.mtx")],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    Y2 = np.loadtxt(tmp_path / "sgtsneEmbedding.txt")
+    assert Y2.shape == (n, 2) and np.isfinite(Y2).all()
