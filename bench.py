@@ -524,7 +524,7 @@ def main():
     ap.add_argument("--spread", type=float, default=60.0)
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--ref-steps", type=int, default=3)
-    ap.add_argument("--relayout", type=int, default=0,
+    ap.add_argument("--relayout", type=int, default=200,
                     help="relabel points along the cell Morton order every R iterations (0 = off)")
     ap.add_argument("--no-expanded", dest="expanded", action="store_false",
                     help="skip the fixed expanded-state (largest grid) line")

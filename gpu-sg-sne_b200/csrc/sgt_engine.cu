@@ -798,26 +798,25 @@ static sgt_status relayout_d(sgt_job *J) {
   CKS(scan_exclusive(J, J->rl_len, n, J->rowptr_alt, J->rowptr_alt + n, s));
   k_relabel_rows<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, s>>>(
       J->rl_p, J->rl_iperm, n, J->rowptr, J->pairs, J->rowptr_alt, J->pairs_alt);
-  // per-point state (all n*S floats): Ynext into the free Y buffer (the next
-  // binning rewrites Y), uY into the free F_rep buffer (the next G2S rewrites
-  // it), gains into its own spare buffer; then swap the roles
+  // per-point state (all n*S floats): Ynext through the free Y buffer (the
+  // next binning rewrites Y), uY through the free F_rep buffer (the next G2S
+  // rewrites it), gains through its own spare buffer.  Everything is copied
+  // back into the job's own buffers, so the captured iteration graphs (which
+  // hold those pointers) stay valid.
+  const size_t vb = sizeof(float) * (size_t)n * J->S;
   k_gather_vec<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, J->rl_p, n, (VT *)J->Y);
   k_gather_vec<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->uY, J->rl_p, n, (VT *)J->Frep);
   k_gather_vec<D><<<nb, SGT_THREADS, 0, s>>>((const VT *)J->gains, J->rl_p, n, (VT *)J->gains_alt);
   CK(cudaGetLastError());
-  std::swap(J->Y, J->Ynext);
-  std::swap(J->uY, J->Frep);
-  std::swap(J->gains, J->gains_alt);
-  std::swap(J->rowptr, J->rowptr_alt);
-  std::swap(J->pairs, J->pairs_alt);
-  if (J->perm) {
-    std::swap(J->perm, J->perm_alt);
-  } else {
-    J->perm = J->perm_alt;
-    J->perm_alt = nullptr;
-    CKS(jalloc(J, &J->perm_alt, (size_t)n));
-  }
-  drop_graphs(J);  // buffers moved: capture the iteration again
+  CK(cudaMemcpyAsync(J->Ynext, J->Y, vb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(J->uY, J->Frep, vb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(J->gains, J->gains_alt, vb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(J->rowptr, J->rowptr_alt, sizeof(int) * ((size_t)n + 1),
+                     cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(J->pairs, J->pairs_alt, sizeof(int2) * (size_t)J->nnz,
+                     cudaMemcpyDeviceToDevice, s));
+  if (!J->perm) CKS(jalloc(J, &J->perm, (size_t)n));
+  CK(cudaMemcpyAsync(J->perm, J->perm_alt, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
   J->relayouts++;
   return SGT_OK;
 }
@@ -1126,27 +1125,39 @@ static sgt_status run_one(sgt_job *J) {
   return SGT_OK;
 }
 
+// `iters` iterations with nothing in between: chained graphs of 16, then
+// single-iteration graphs
+static sgt_status run_chunk(sgt_job *J, int iters) {
+  sgt_ctx *ctx = J->ctx;
+  int left = iters;
+  if (left >= SGT_GRAPH_ITERS && !J->gexec_multi)
+    CKS(instantiate(J, SGT_GRAPH_ITERS, &J->gexec_multi));
+  for (; left >= SGT_GRAPH_ITERS; left -= SGT_GRAPH_ITERS)
+    CK(cudaGraphLaunch(J->gexec_multi, ctx->stream));
+  for (; left > 0; left--) CKS(run_one(J));
+  return SGT_OK;
+}
+
 sgt_status sgt_job_run(sgt_job *J, int iters) {
   if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
   sgt_ctx *ctx = J->ctx;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
-  const int every = J->p.relayout_every;
-  if (every <= 0 && J->p.kl_every <= 0) {
-    // nothing happens between iterations: chained graphs of 16 iterations
-    int left = iters;
-    if (left >= SGT_GRAPH_ITERS && !J->gexec_multi)
-      CKS(instantiate(J, SGT_GRAPH_ITERS, &J->gexec_multi));
-    for (; left >= SGT_GRAPH_ITERS; left -= SGT_GRAPH_ITERS) CK(cudaGraphLaunch(J->gexec_multi, s));
-    for (; left > 0; left--) CKS(run_one(J));
-    J->host_iter += iters;
-    return SGT_OK;
-  }
-  for (int it = 0; it < iters; it++) {
+  (void)s;
+  const int every = J->p.relayout_every, kl_every = J->p.kl_every;
+  // runs of iterations between the points where host work happens (a
+  // relayout before every `every`-th iteration, a KL after every
+  // `kl_every`-th), each run through the chained graphs
+  int left = iters;
+  while (left > 0) {
     if (every > 0 && J->host_iter > 0 && J->host_iter % every == 0) CKS(relayout(J));
-    CKS(run_one(J));
-    J->host_iter++;
-    if (J->p.kl_every > 0 && (J->host_iter % J->p.kl_every) == 0) {
+    int run = left;
+    if (every > 0) run = std::min(run, every - (int)(J->host_iter % every));
+    if (kl_every > 0) run = std::min(run, kl_every - (int)(J->host_iter % kl_every));
+    CKS(run_chunk(J, run));
+    J->host_iter += run;
+    left -= run;
+    if (kl_every > 0 && (J->host_iter % kl_every) == 0) {
       double kl = 0;
       // KL of the coordinates the step just used (Y) with that step's Z
       CKS(sgt_job_kl(J, -1.0, &kl));
