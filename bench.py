@@ -353,6 +353,11 @@ def run_ours(args, rank, world, local, dist):
         ratio = read_traffic(nnz, n)
         # bin count/scan/scatter, s2g (tile + cell), fft x3, g2s, SpMV, combine
         per_iter_kernels = 11
+        # a relayout before every R-th iteration: cell keys, two 3-kernel
+        # scans, key scatter, permutation prep, row relabel, 3 gathers
+        R = args.relayout
+        relayouts = 0 if R <= 0 else (W + K - 1) // R - (W - 1) // R
+        launches = per_iter_kernels * K + 13 * relayouts
         value = world * K / (ms / 1e3)
         out = {
             "metric": METRIC, "value": value, "unit": "iters/s",
@@ -385,7 +390,7 @@ def run_ours(args, rank, world, local, dist):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "includes": "job create from pinned host CSR, H2D of P and Y0, "
                                 f"{W + K} iterations, D2H of Y"},
-            "gpu_launches": per_iter_kernels * K,
+            "gpu_launches": launches,
             "clocks": clk,
             "batched": batched,
             "served": served,

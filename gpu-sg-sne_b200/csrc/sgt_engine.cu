@@ -857,7 +857,6 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   if (nnz <= 0) return fail(ctx, SGT_ERR_INVALID_ARG, "P has no nonzeros");
   std::vector<int> hcol;
   std::vector<float> hval;
-  const bool need_host = !mem_is_device || params->format == SGT_FORMAT_HYBRID;
   if (mem_is_device) {
     if (params->format == SGT_FORMAT_HYBRID) {
       hcol.resize(nnz);
@@ -870,7 +869,6 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   } else {
     CKS(check_csr(ctx, n, hrp.data(), col));
   }
-  (void)need_host;
   if (mem_is_device && params->format != SGT_FORMAT_HYBRID) {
     int *bad = nullptr;
     CK(cudaMallocAsync(&bad, sizeof(int), s));
@@ -1142,8 +1140,6 @@ sgt_status sgt_job_run(sgt_job *J, int iters) {
   if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
   sgt_ctx *ctx = J->ctx;
   CK(cudaSetDevice(ctx->device));
-  cudaStream_t s = ctx->stream;
-  (void)s;
   const int every = J->p.relayout_every, kl_every = J->p.kl_every;
   // runs of iterations between the points where host work happens (a
   // relayout before every `every`-th iteration, a KL after every

@@ -198,3 +198,47 @@ def test_server_budget_and_oversize(problems):
             tiny.close()
     assert e.value.status == 3
     srv.close()
+
+
+def test_one_dimensional_batch_and_server(problems):
+    """d = 1 jobs (and a COO and a hybrid one) in a batch and through the
+    server: the same after two iterations as alone."""
+    import sgtsne_b200 as S
+    ctx = S.Context(0)
+    probs = []
+    for fmt, (rp, col, val, _, y0) in zip((0, 2, 3), problems[:3]):
+        probs.append((rp, col, val, y0[:, :1].copy(), fmt))
+
+    def par(fmt, it):
+        return S.default_params(d=1, format=fmt, max_iter=it, early_iter=EARLY, h=0.5)
+    alone = []
+    for rp, col, val, y0, fmt in probs:
+        j = S.Job(ctx, par(fmt, SHORT), rp, col, val, device_mem=False)
+        j.set_y(y0, S.LAYOUT_POINT_MAJOR, False)
+        j.run(SHORT)
+        alone.append(j.get_y(np.empty_like(y0), S.LAYOUT_POINT_MAJOR, False, 1))
+        j.close()
+    jobs = []
+    for rp, col, val, y0, fmt in probs:
+        j = S.Job(ctx, par(fmt, SHORT), rp, col, val, device_mem=False)
+        j.set_y(y0, S.LAYOUT_POINT_MAJOR, False)
+        jobs.append(j)
+    b = S.Batch(ctx, jobs, iters_per_launch=4)
+    b.run(SHORT)
+    for j, ref in zip(jobs, alone):
+        assert rel(j.get_y(np.empty_like(ref), S.LAYOUT_POINT_MAJOR, False, 1), ref) <= TOL_Y
+    b.close()
+    for j in jobs:
+        j.close()
+    ctx.close()
+    srv = S.Server(0, max_active=2, iters_per_round=4)
+    outs = [srv.submit(par(fmt, SHORT), rp, col, val, y0)[1] for rp, col, val, y0, fmt in probs]
+    done = []
+    for _ in range(300):
+        done += srv.poll(wait_ms=50)
+        if len(done) == len(probs):
+            break
+    for r, (out, ref) in enumerate(zip(outs, alone)):
+        assert srv.info(r).state == S.REQ_DONE
+        assert rel(out, ref) <= TOL_Y
+    srv.close()

@@ -557,3 +557,63 @@ def test_cli_dense_and_mtx(torch, ctx, oracle, tmp_path):
     assert r.returncode == 0, r.stderr
     Y2 = np.loadtxt(tmp_path / "sgtsneEmbedding.txt")
     assert Y2.shape == (n, 2) and np.isfinite(Y2).all()
+
+
+@pytest.mark.parametrize("fmt", [0, 2, 3])
+def test_ragged_p_iterations(torch, ctx, oracle, fmt):
+    """P with empty rows and single-entry rows (isolated and leaf points)
+    through 60 iterations in each format: finite, the isolated points feel
+    only repulsion, and the run stays within 1 % KL of the oracle's."""
+    import sgtsne_b200 as S
+    rp, col, val, _ = make_problem(n=2000, k=10, seed=77)
+    n = len(rp) - 1
+    lens = np.diff(rp).copy()
+    keep = np.ones(int(rp[-1]), bool)
+    empty = np.arange(0, n, 97)          # rows emptied
+    for r in empty:
+        keep[rp[r]:rp[r + 1]] = False
+    single = np.arange(50, n, 101)       # rows cut to one entry
+    for r in single:
+        keep[rp[r] + 1:rp[r + 1]] = False
+    lens = np.add.reduceat(keep.astype(np.int64), rp[:-1]) * (lens > 0)
+    rp2 = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    col2, val2 = col[keep], val[keep].astype(np.float32)
+    Y0 = (np.random.default_rng(8).standard_normal((n, 2)) * 1e-2).astype(np.float32)
+    p = S.default_params(d=2, format=fmt, max_iter=60, early_iter=20)
+    job = S.Job(ctx, p, rp2, col2, val2, device_mem=False)
+    job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+    job.run(60)
+    Y = job.get_y(np.empty((n, 2), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+    assert job.info().error_flags == 0
+    job.close()
+    assert np.isfinite(Y).all()
+    Yo = oracle.kl_minimization(rp2, col2, val2.astype(np.float64), Y0.astype(np.float64), 60,
+                                early_iter=20, alpha=12.0, h=0.7, grid_mode=0)
+    kls = []
+    for Yx in (Y.astype(np.float64), Yo):
+        _, Z, _, _ = oracle.repulsive_interp(Yx, 0.7)
+        kls.append(oracle.kl(rp2, col2, val2.astype(np.float64), Yx, 1.0, Z))
+    assert abs(kls[0] - kls[1]) <= 0.01 * kls[1]
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_smallest_embeddings(torch, ctx, d):
+    """n = 3 and n = 40 points: every stage runs with one block and the
+    result stays finite.  So few points repel each other far apart, so a 3-D
+    run may outgrow the largest grid the job allocated: the engine then
+    clamps the grid and says so (flag 2), which is allowed here; non-finite
+    values (1) and chunk overflow (4) are not."""
+    import sgtsne_b200 as S
+    for n in (3, 40):
+        rng = np.random.default_rng(n + d)
+        rp = np.arange(0, 2 * (n + 1), 2, dtype=np.int32)
+        col = np.stack([(np.arange(n) + 1) % n, (np.arange(n) + 2) % n], 1).reshape(-1)
+        val = np.full(2 * n, 0.5 / n, np.float32)
+        Y0 = (rng.standard_normal((n, d)) * 1e-2).astype(np.float32)
+        job = S.Job(ctx, S.default_params(d=d, format=S.FORMAT_CSR), rp, col.astype(np.int32),
+                    val, device_mem=False)
+        job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+        job.run(40)
+        Y = job.get_y(np.empty((n, d), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        assert (job.info().error_flags & ~2) == 0 and np.isfinite(Y).all()
+        job.close()
