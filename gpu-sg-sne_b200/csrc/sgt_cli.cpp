@@ -14,13 +14,17 @@
 // ceil(3u) neighbours (sgt_knn, where the reference calls FLANN), distances
 // divided by their maximum, perplexity equalisation to u (sgt_perplexity),
 // then sgt_embed.
-// Outputs: sgtsneEmbedding.txt (one point per line) and timeInfo.txt.
+// Initial coordinates come from yin2m.txt in the working directory when it
+// exists (as the reference's demo), else 1e-4 N(0,1).
+// Outputs: sgtsneEmbedding.txt (one point per line, as extractEmbeddingTextT)
+// and timeInfo.txt (appended, as ExtractTimeInfo).
 #include "sgtsne_b200.h"
 
 #include <cuda_runtime.h>
 #include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -227,7 +231,26 @@ int main(int argc, char **argv) {
   p.n = n;
   std::vector<float> y((size_t)n * (p.d > 0 ? p.d : 2));
   std::vector<double> timeinfo(7003, 0.0);
-  st = sgt_embed(ctx, n, rp.data(), col.data(), val.data(), &p, nullptr, y.data(), timeinfo.data());
+  // initial coordinates from yin2m.txt when it exists (one point per line,
+  // stored dim-major), as demo_perplexity.cu:175-185; random otherwise
+  std::vector<float> yin;
+  {
+    std::ifstream yinf("yin2m.txt");
+    if (yinf) {
+      yin.resize((size_t)n * p.d);
+      bool ok = true;
+      for (int i = 0; i < n && ok; i++)
+        for (int j = 0; j < p.d && ok; j++) ok = (bool)(yinf >> yin[i + (size_t)j * n]);
+      if (!ok) {
+        std::cerr << "yin2m.txt holds fewer than n*d values; using random Y0" << std::endl;
+        yin.clear();
+      }
+    }
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  st = sgt_embed(ctx, n, rp.data(), col.data(), val.data(), &p, yin.empty() ? nullptr : yin.data(),
+                 y.data(), timeinfo.data());
+  timeinfo[7002] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (st != SGT_OK) {
     std::cerr << "sgt_embed: " << sgt_status_string(st) << ": " << sgt_last_error(ctx) << std::endl;
     sgt_destroy(ctx);
@@ -241,11 +264,19 @@ int main(int argc, char **argv) {
     }
   }
   {
-    std::ofstream f("timeInfo.txt");
-    f << "total_ms " << timeinfo[7000] << "\nsetup_ms " << timeinfo[7001] << "\nzeta "
+    // appended in the layout of ExtractTimeInfo (CU/utils.cu:72-92); the
+    // reference writes only when the file already exists, this tool always
+    std::ofstream f("timeInfo.txt", std::ios::app);
+    f << "N d gds matrix total: \n";
+    f << n << " " << p.d << " " << timeinfo[7000] << " " << timeinfo[7001] << " "
       << timeinfo[7002] << "\n";
+    f << "Fattr S2G G2G G2S Phi2F Nuconv Pre";
+    for (int i = 0; i < 1000; i++) {
+      for (int j = 0; j < 7; j++) f << timeinfo[i * 7 + j] << " ";
+      f << "\n";
+    }
   }
-  printf("time=%lf\n", timeinfo[7000]);
+  printf("Total time=%lf\n", timeinfo[7002]);
   sgt_destroy(ctx);
   return 0;
 }

@@ -111,8 +111,10 @@ const char *sgt_last_error(const sgt_ctx *ctx);
  * y_in: host, dim-major n*d, or NULL for 1e-4 * N(0,1) from
  * std::default_random_engine (CU/utils.cu:185-193).  y_out: host, dim-major
  * n*d, caller-owned (the reference returned a malloc'd array).
- * time_info: NULL or >= 7003 doubles; [7000] = total ms, [7001] = setup ms,
- * [7002] = Z of the last iteration. */
+ * time_info: NULL or >= 7003 doubles; as the reference, [7000] = gradient
+ * descent ms, [7001] = preparation of P ms, [7002] = whole call ms; the
+ * per-iteration stage slots [7 i + j] are left as given (iterations run as
+ * captured graphs; sgt_job_profile measures stages). */
 sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const int *col,
                      const float *val, const sgt_params *params,
                      const float *y_in, float *y_out, double *time_info);

@@ -557,6 +557,19 @@ def test_cli_dense_and_mtx(torch, ctx, oracle, tmp_path):
     assert r.returncode == 0, r.stderr
     Y2 = np.loadtxt(tmp_path / "sgtsneEmbedding.txt")
     assert Y2.shape == (n, 2) and np.isfinite(Y2).all()
+    # timeInfo.txt in the reference's layout, one block per run (two runs so far)
+    lines = (tmp_path / "timeInfo.txt").read_text().splitlines()
+    assert lines.count("N d gds matrix total: ") == 2
+    assert len(lines[1].split()) == 5 and lines[1].split()[:2] == [str(n), "2"]
+    # Y0 from yin2m.txt (one point per line): with no iteration the result is
+    # Y0 minus its mean
+    Yin = np.random.default_rng(4).standard_normal((n, 2)).astype(np.float32)
+    np.savetxt(tmp_path / "yin2m.txt", Yin, fmt="%.9g")
+    r = subprocess.run([exe, "-d", "2", "-m", "0", "-t", "csr", str(tmp_path / "p.mtx")],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    Y3 = np.loadtxt(tmp_path / "sgtsneEmbedding.txt")
+    assert np.abs(Y3 - (Yin - Yin.mean(0))).max() <= 1e-5
 
 
 @pytest.mark.parametrize("fmt", [0, 2, 3])
