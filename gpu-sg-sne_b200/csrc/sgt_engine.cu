@@ -267,6 +267,53 @@ static sgt_status check_csr(sgt_ctx *ctx, int n, const int *rowptr, const int *c
   return SGT_OK;
 }
 
+// CSR -> ELL (column-major, zero padded) + COO tail in row order on the
+// device, given the row pointers on the host too (for the tail offsets).
+// The same layout as sgt_csr_to_hybrid (CU/prepareMatrix.cu:55-97).
+__global__ void k_csr_to_hybrid(int n, int w, const int *__restrict__ rowptr,
+                                const int *__restrict__ col, const float *__restrict__ val,
+                                const long *__restrict__ tail, unsigned *__restrict__ ell_cols,
+                                float *__restrict__ ell_vals, unsigned *__restrict__ coo_rows,
+                                unsigned *__restrict__ coo_cols, float *__restrict__ coo_vals) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int s0 = rowptr[r], len = rowptr[r + 1] - s0;
+    for (int k = 0; k < w; k++) {  // consecutive rows write consecutive slots
+      const bool in = k < len;
+      ell_cols[(size_t)k * n + r] = in ? (unsigned)col[s0 + k] : 0u;
+      ell_vals[(size_t)k * n + r] = in ? val[s0 + k] : 0.f;
+    }
+    const long t0 = tail[r];
+    for (int k = w; k < len; k++) {
+      coo_rows[t0 + k - w] = (unsigned)r;
+      coo_cols[t0 + k - w] = (unsigned)col[s0 + k];
+      coo_vals[t0 + k - w] = val[s0 + k];
+    }
+  }
+}
+
+static sgt_status hybrid_split_device(sgt_ctx *ctx, int n, const std::vector<int> &hrp,
+                                      const int *rowptr, const int *col, const float *val, int w,
+                                      unsigned *ell_cols, float *ell_vals, unsigned *coo_rows,
+                                      unsigned *coo_cols, float *coo_vals, long *coo_size) {
+  cudaStream_t s = ctx->stream;
+  std::vector<long> tail((size_t)n + 1, 0);
+  for (int r = 0; r < n; r++) tail[r + 1] = tail[r] + std::max(0, hrp[r + 1] - hrp[r] - w);
+  long *dt = nullptr;
+  CK(cudaMallocAsync(&dt, sizeof(long) * ((size_t)n + 1), s));
+  cudaError_t e = cudaMemcpyAsync(dt, tail.data(), sizeof(long) * ((size_t)n + 1),
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    k_csr_to_hybrid<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(
+        n, w, rowptr, col, val, dt, ell_cols, ell_vals, coo_rows, coo_cols, coo_vals);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host tail array is freed next
+  cudaFreeAsync(dt, s);
+  CK(e);
+  *coo_size = tail[n];
+  return SGT_OK;
+}
+
 static int choose_group(long nnz, int n) {
   const double avg = n > 0 ? (double)nnz / n : 0.0;
   if (avg <= 6) return 4;
@@ -855,21 +902,8 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   }
   const long nnz = hrp[n];
   if (nnz <= 0) return fail(ctx, SGT_ERR_INVALID_ARG, "P has no nonzeros");
-  std::vector<int> hcol;
-  std::vector<float> hval;
+  if (!mem_is_device) CKS(check_csr(ctx, n, hrp.data(), col));
   if (mem_is_device) {
-    if (params->format == SGT_FORMAT_HYBRID) {
-      hcol.resize(nnz);
-      hval.resize(nnz);
-      CK(cudaMemcpyAsync(hcol.data(), col, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(hval.data(), val, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      CKS(check_csr(ctx, n, hrp.data(), hcol.data()));
-    }
-  } else {
-    CKS(check_csr(ctx, n, hrp.data(), col));
-  }
-  if (mem_is_device && params->format != SGT_FORMAT_HYBRID) {
     int *bad = nullptr;
     CK(cudaMallocAsync(&bad, sizeof(int), s));
     CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
@@ -948,9 +982,25 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
       cudaFreeAsync(dcol, s);
       cudaFreeAsync(dval, s);
     }
-  } else {  // hybrid: host split like CU/prepareMatrix.cu:55-97
-    const int *hc = mem_is_device ? hcol.data() : col;
-    const float *hv = mem_is_device ? hval.data() : val;
+  } else if (mem_is_device) {  // hybrid from device arrays: split on the device
+    const int w = sgt_ell_width(n, hrp.data());
+    long csz = 0;
+    for (int r = 0; r < n; r++) csz += std::max(0, hrp[r + 1] - hrp[r] - w);
+    J->ell_w = w;
+    J->coo_n = csz;
+    if ((st = jalloc(J, &J->ell_cols, (size_t)n * std::max(w, 1))) != SGT_OK ||
+        (st = jalloc(J, &J->ell_vals, (size_t)n * std::max(w, 1))) != SGT_OK ||
+        (st = jalloc(J, &J->coo_rows, (size_t)std::max(csz, 1L))) != SGT_OK ||
+        (st = jalloc(J, &J->coo_cols, (size_t)std::max(csz, 1L))) != SGT_OK ||
+        (st = jalloc(J, &J->coo_vals, (size_t)std::max(csz, 1L))) != SGT_OK)
+      return bail(st);
+    long got = 0;
+    if ((st = hybrid_split_device(ctx, n, hrp, rowptr, col, val, w, J->ell_cols, J->ell_vals,
+                                  J->coo_rows, J->coo_cols, J->coo_vals, &got)) != SGT_OK)
+      return bail(st);
+  } else {  // hybrid from host arrays: host split like CU/prepareMatrix.cu:55-97
+    const int *hc = col;
+    const float *hv = val;
     const int w = sgt_ell_width(n, hrp.data());
     std::vector<unsigned> ec((size_t)n * std::max(w, 1)), cr(nnz), cc(nnz);
     std::vector<float> ev((size_t)n * std::max(w, 1)), cv(nnz);
@@ -2005,4 +2055,25 @@ extern "C" sgt_status sgt_repulsive_noalloc(sgt_ctx *ctx, int n, int d, float h,
   if (h_eff) *h_eff = hs.h_eff;
   if (hs.error & SGT_EFLAG_NONFINITE) return fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates");
   return SGT_OK;
+}
+
+// CSR -> ELL + COO on the device (the device twin of sgt_csr_to_hybrid)
+extern "C" sgt_status sgt_csr_to_hybrid_device(sgt_ctx *ctx, int n, const int *rowptr,
+                                               const int *col, const float *val, int width,
+                                               unsigned *ell_cols, float *ell_vals,
+                                               unsigned *coo_rows, unsigned *coo_cols,
+                                               float *coo_vals, long *coo_size) {
+  if (!ctx || n < 1 || width < 0 || !rowptr || !col || !val || !coo_size ||
+      !coo_rows || !coo_cols || !coo_vals || (width > 0 && (!ell_cols || !ell_vals)))
+    return SGT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<int> hrp((size_t)n + 1);
+  CK(cudaMemcpyAsync(hrp.data(), rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (hrp[0] != 0) return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr[0] must be 0");
+  for (int r = 0; r < n; r++)
+    if (hrp[r + 1] < hrp[r]) return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr must not decrease");
+  return hybrid_split_device(ctx, n, hrp, rowptr, col, val, width, ell_cols, ell_vals, coo_rows,
+                             coo_cols, coo_vals, coo_size);
 }

@@ -116,6 +116,8 @@ SIGNATURES = {
     "sgt_symmetrize": (_i, [_i, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_symmetrize_device": (_i, [_vp, _i, _l, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_knn": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp]),
+    "sgt_csr_to_hybrid_device": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp,
+                                      C.POINTER(_l)]),
 }
 
 _LIB = None
@@ -243,6 +245,16 @@ class Context:
         into device idx/d2 (n*k)."""
         self.check(self.lib.sgt_knn(self.h, int(n), int(dim), _ptr(X), int(k), _ptr(idx),
                                     _ptr(d2)), "knn")
+
+    def csr_to_hybrid(self, n, rowptr, col, val, width, ell_cols, ell_vals, coo_rows,
+                      coo_cols, coo_vals):
+        """CSR -> ELL + COO on the device; returns the COO tail length."""
+        k = C.c_long()
+        self.check(self.lib.sgt_csr_to_hybrid_device(
+            self.h, int(n), _ptr(rowptr), _ptr(col), _ptr(val), int(width), _ptr(ell_cols),
+            _ptr(ell_vals), _ptr(coo_rows), _ptr(coo_cols), _ptr(coo_vals), C.byref(k)),
+            "csr_to_hybrid_device")
+        return k.value
 
     def symmetrize(self, n, nnz, rowptr, col, val, scale, out_rowptr, out_col, out_val):
         """(P + P^T) * scale on the device; out_col/out_val hold 2 nnz.

@@ -353,6 +353,15 @@ sgt_status sgt_symmetrize_device(sgt_ctx *ctx, int n, long nnz, const int *rowpt
                                  int *out_rowptr, int *out_col, float *out_val,
                                  long *out_nnz);
 
+/* The same split on the device: device arrays (ell_* sized n*width, coo_*
+   sized nnz); *coo_size receives the tail length (synchronises).
+   Bit-identical to sgt_csr_to_hybrid. */
+sgt_status sgt_csr_to_hybrid_device(sgt_ctx *ctx, int n, const int *rowptr,
+                                    const int *col, const float *val, int width,
+                                    unsigned *ell_cols, float *ell_vals,
+                                    unsigned *coo_rows, unsigned *coo_cols,
+                                    float *coo_vals, long *coo_size);
+
 /* (P + P^T) * scale with sorted columns per row (CU/graph_rescaling.cu:266-398
    uses scale 1/(2n)).  Host arrays.  Call with out_col == NULL to get
    *out_nnz, then again with out arrays of that size. */
