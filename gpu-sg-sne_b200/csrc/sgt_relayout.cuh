@@ -1,8 +1,8 @@
 // sgt_relayout.cuh -- locality relabelling of an embedding.
 //
 // t-SNE places graph neighbours close together, so once the embedding has
-// structure, ordering the points along a space-filling curve of their grid
-// cells makes the neighbours of consecutive rows consecutive in memory: the
+// structure, ordering the points along a space-filling curve of fine cells
+// makes the neighbours of consecutive rows consecutive in memory: the
 // coordinate gathers of the row kernel then hit L1 instead of L2.  Every R
 // iterations the engine counting-sorts the points by the Morton code of their
 // cell and rewrites P symmetrically in that order (columns remapped, each
@@ -30,14 +30,18 @@ __device__ __forceinline__ unsigned spread3(unsigned x) {  // 10 bits -> every t
   return x;
 }
 
-// cell key of every point of Ynext under the grid decision of the next
-// binning (2-D: Morton of the 512x512 cells, 18 bits; 3-D: Morton of cells
-// coarsened to 64^3, 18 bits; 1-D: the cell).
+// key of every point of Ynext: the Morton code of its cell in a fine
+// lattice over the bounding box of the next binning (2-D: 512 x 512 cells;
+// 3-D: 64^3 cells; 1-D: 2^18 cells; 18 bits in each case).  The lattice is
+// far finer than the interpolation grid (16-25 points per axis in a typical
+// run), so a cell holds a handful of points and graph neighbours that lie
+// close in the embedding also lie close in memory.
 template <int D>
 __global__ void k_cell_keys(const typename Vec<D>::T *__restrict__ Ynext, int n,
                             const SgtState *st, unsigned *__restrict__ keys,
                             int *__restrict__ hist) {
-  const float maxy = st->maxy, scale = st->scale;
+  const float maxy = st->maxy;
+  const float res = D == 1 ? 262144.f : D == 2 ? 512.f : 64.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const typename Vec<D>::T y = Ynext[i];
     unsigned f[3] = {0, 0, 0};
@@ -45,12 +49,13 @@ __global__ void k_cell_keys(const typename Vec<D>::T *__restrict__ Ynext, int n,
     for (int k = 0; k < D; k++) {
       float sh;
       const float yc = __fsub_rn(comp<D>(y, k), st->mean[k]);
-      f[k] = (unsigned)floorf(sgt_scale(yc, st->miny[k], maxy, scale, sh));
+      const float v = fmaxf(floorf(sgt_scale(yc, st->miny[k], maxy, res, sh)), 0.f);
+      f[k] = min((unsigned)v, (unsigned)res - 1u);
     }
     unsigned key;
     if (D == 1) key = f[0];
     else if (D == 2) key = spread2(f[0]) | (spread2(f[1]) << 1);
-    else key = spread3(f[0] >> 2) | (spread3(f[1] >> 2) << 1) | (spread3(f[2] >> 2) << 2);
+    else key = spread3(f[0]) | (spread3(f[1]) << 1) | (spread3(f[2]) << 2);
     keys[i] = key;
     atomicAdd(&hist[key], 1);
   }
