@@ -25,6 +25,7 @@ REPO = os.path.abspath(os.path.join(PKG_DIR, ".."))
 HEADER = os.path.join(REPO, "include", "sgtsne_b200.h")
 
 FORMAT_CSR, FORMAT_COO, FORMAT_HYBRID = 0, 2, 3
+KNN_AUTO, KNN_SIMT, KNN_TENSOR = 0, 1, 2
 LAYOUT_DIM_MAJOR, LAYOUT_POINT_MAJOR = 0, 1
 GRID_H, GRID_FIXED = 0, 1
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
@@ -116,6 +117,7 @@ SIGNATURES = {
     "sgt_symmetrize": (_i, [_i, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_symmetrize_device": (_i, [_vp, _i, _l, _vp, _vp, _vp, _f, _vp, _vp, _vp, C.POINTER(_l)]),
     "sgt_knn": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp]),
+    "sgt_knn_ex": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp, _i, C.POINTER(_i)]),
     "sgt_csr_to_hybrid_device": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp,
                                       C.POINTER(_l)]),
 }
@@ -240,11 +242,19 @@ class Context:
         self.check(self.lib.sgt_perplexity(self.h, n, k, _ptr(dist), float(perp), _ptr(p),
                                            _ptr(beta)), "perplexity")
 
-    def knn(self, n, dim, X, k, idx, d2):
+    def knn(self, n, dim, X, k, idx, d2, method=None):
         """Exact kNN (squared distances, self excluded) of device X (n*dim)
-        into device idx/d2 (n*k)."""
-        self.check(self.lib.sgt_knn(self.h, int(n), int(dim), _ptr(X), int(k), _ptr(idx),
-                                    _ptr(d2)), "knn")
+        into device idx/d2 (n*k).  method: None (sgt_knn) or KNN_AUTO /
+        KNN_SIMT / KNN_TENSOR (sgt_knn_ex); with a method, returns the number
+        of queries the tensor-core filter handed to the SIMT search."""
+        if method is None:
+            self.check(self.lib.sgt_knn(self.h, int(n), int(dim), _ptr(X), int(k), _ptr(idx),
+                                        _ptr(d2)), "knn")
+            return None
+        redo = C.c_int()
+        self.check(self.lib.sgt_knn_ex(self.h, int(n), int(dim), _ptr(X), int(k), _ptr(idx),
+                                       _ptr(d2), int(method), C.byref(redo)), "knn_ex")
+        return redo.value
 
     def csr_to_hybrid(self, n, rowptr, col, val, width, ell_cols, ell_vals, coo_rows,
                       coo_cols, coo_vals):

@@ -343,6 +343,21 @@ sgt_status sgt_csr_to_hybrid(int n, const int *rowptr, const int *col,
 sgt_status sgt_knn(sgt_ctx *ctx, int n, int dim, const float *X, int k, int *idx,
                    float *d2);
 
+/* Search methods of sgt_knn_ex; all return the same bits.
+   SGT_KNN_SIMT: sums of squared differences, one query per thread.
+   SGT_KNN_TENSOR: dim <= 64 and k <= 32 only.  Distances
+     |q|^2 + |c|^2 - 2 q.c of all pairs on the tensor cores (TF32 in three
+     terms, FP32 accumulation) keep a list of 64 candidates per query,
+     re-ranked with the SIMT arithmetic; queries whose list could miss a
+     neighbour under the filter's error bound are redone by the SIMT search.
+   SGT_KNN_AUTO: the tensor-core filter where it applies and n >= 4096. */
+enum { SGT_KNN_AUTO = 0, SGT_KNN_SIMT = 1, SGT_KNN_TENSOR = 2 };
+
+/* sgt_knn with a method; *n_redo (may be NULL) receives the number of
+   queries the tensor-core filter handed to the SIMT search. */
+sgt_status sgt_knn_ex(sgt_ctx *ctx, int n, int dim, const float *X, int k, int *idx,
+                      float *d2, int method, int *n_redo);
+
 /* The same on the device: device arrays, out_col/out_val sized 2*nnz (an
    upper bound), out_rowptr n+1; *out_nnz receives the count (synchronises
    the context's stream).  Bit-identical to sgt_symmetrize.  n <= 2^24,

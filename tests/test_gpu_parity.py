@@ -563,6 +563,53 @@ def test_knn_exact(torch, ctx, n, dim, k):
     assert np.abs(Dchk - Dg).max() <= 1e-5 * max(Dref.max(), 1.0)
 
 
+@pytest.mark.parametrize("n,dim,k,kind", [(20000, 50, 30, "zipf"), (9999, 7, 15, "blobs"),
+                                          (6000, 64, 32, "blobs"), (5000, 33, 1, "blobs"),
+                                          (4500, 2, 10, "grid"), (300, 16, 10, "blobs"),
+                                          (60, 8, 5, "blobs")])
+def test_knn_tensor_filter_matches_simt(torch, ctx, n, dim, k, kind):
+    """The tensor-core filter (TF32 in three terms, exact re-rank, SIMT redo
+    of unsettled queries) against the SIMT search: the same indices and the
+    same distance bits.  'zipf' is the 50-D generator of the 1.3M-point
+    configuration; 'grid' puts points on an integer lattice, so distances
+    tie everywhere and the ties must resolve by index as in the SIMT
+    search."""
+    import sgtsne_b200 as S
+    from sgtsne_b200 import workloads as W
+    rng = np.random.default_rng(n + dim)
+    if kind == "zipf":
+        X, _ = W.gmm_zipf(n, dim=dim, ncomp=40, zipf_a=1.1, centre_var=25.0, seed=3)
+    elif kind == "grid":
+        X = rng.integers(0, 40, (n, dim)).astype(np.float32)
+    else:
+        c = rng.standard_normal((8, dim)) * 4
+        X = (c[rng.integers(0, 8, n)] + rng.standard_normal((n, dim))).astype(np.float32)
+    X = np.ascontiguousarray(X, np.float32)
+    out = {}
+    for m in (S.KNN_SIMT, S.KNN_TENSOR):
+        idx = torch.full((n * k,), -7, dtype=torch.int32, device="cuda")
+        d2 = torch.full((n * k,), -7.0, dtype=torch.float32, device="cuda")
+        redo = ctx.knn(n, dim, dev(torch, X), k, idx, d2, method=m)
+        out[m] = (idx.cpu().numpy(), d2.cpu().numpy(), redo)
+    (i1, d1, _), (i2, dd2, redo) = out[S.KNN_SIMT], out[S.KNN_TENSOR]
+    print(f"\nknn n={n} dim={dim} k={k} {kind}: {redo} of {n} queries redone by the SIMT search")
+    assert np.array_equal(i1, i2)
+    assert np.array_equal(d1.view(np.uint32), dd2.view(np.uint32))
+    if kind != "grid":
+        assert redo <= 0.01 * n
+
+
+def test_knn_tensor_rejects_wide_points_and_large_k(torch, ctx):
+    import sgtsne_b200 as S
+    X = torch.zeros(5000 * 65, dtype=torch.float32, device="cuda")
+    idx = torch.empty(5000 * 40, dtype=torch.int32, device="cuda")
+    d2 = torch.empty(5000 * 40, dtype=torch.float32, device="cuda")
+    for dim, k in ((65, 4), (20, 33)):
+        with pytest.raises(S.SgtError) as e:
+            ctx.knn(5000, dim, X, k, idx, d2, method=S.KNN_TENSOR)
+        assert e.value.status == 4
+
+
 def test_knn_rejects_bad_k(torch, ctx):
     import sgtsne_b200 as S
     X = torch.zeros(10 * 3, dtype=torch.float32, device="cuda")
