@@ -233,10 +233,13 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, float *v) {
 }
 
 // hi/lo images of every 128-point block in its two roles ([block][part]
-// [unit][row] float4; rows past n and unused dimensions are zero), and the
-// squared norms (FP32, dimension order) with their maximum.  A query row is
+// [unit][row] float4; unused dimensions are zero), and the squared norms
+// (FP32, dimension order) with their maximum.  A query row is
 // (x, 1, -|x|^2/2) and a candidate row (x, -|x|^2/2, 1) in dimensions
 // dim and dim + 1, so one product is q.c - (|q|^2 + |c|^2)/2 = -d^2/2.
+// Query rows past n are zero; candidate rows past n are (0, -1e30, 0), at
+// distance 2e30 from every query, so they are admitted only while a list is
+// not yet full and sort after every real candidate.
 __global__ void k_knn_norms(const float *__restrict__ X, int n, int dim, float *__restrict__ nrm,
                             unsigned *__restrict__ nmax) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -261,7 +264,7 @@ __global__ void k_knn_split(const float *__restrict__ X, const float *__restrict
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const int kk = 4 * u + c;
-      float x = 0.f, ya = 0.f, yb = 0.f;
+      float x = 0.f, ya = 0.f, yb = (i >= n && kk == dim) ? -1e30f : 0.f;
       if (i < n) {
         if (kk < dim) {
           x = X[(long)i * dim + kk];
@@ -309,6 +312,7 @@ struct TcList {
   int j[KNN_TC_CAP];
   float thr;  // largest entry (distance, index) and its slot
   int thi, mp;
+  float mthr;  // -thr/2: a tile value v (= -d^2/2) admits its candidate when v > mthr
   __device__ __forceinline__ void init() {
 #pragma unroll
     for (int e = 0; e < KNN_TC_CAP; e++) {
@@ -318,6 +322,7 @@ struct TcList {
     thr = INFINITY;
     thi = 0x7fffffff;
     mp = 0;
+    mthr = -INFINITY;
   }
   __device__ __forceinline__ void offer(float dd, int jj) {
     if (!knn_less(dd, jj, thr, thi)) return;
@@ -337,6 +342,7 @@ struct TcList {
         thi = j[e];
         mp = e;
       }
+    mthr = -0.5f * thr;
   }
 };
 
@@ -398,7 +404,10 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
   const float qn = q < n ? nrm[q] : 0.f;
   TcList L;
   L.init();
-  if (q >= n) L.thr = -INFINITY;  // admits nothing
+  if (q >= n) {  // admits nothing
+    L.thr = -INFINITY;
+    L.mthr = INFINITY;
+  }
   // queue of candidates that beat the threshold (local memory, written
   // rarely): drained, by the whole warp at once, once a thread could
   // overflow it during the next 32 columns
@@ -415,15 +424,17 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
         cpend[st] = false;
         tc_fence_after();
         const unsigned dt = tmem + (unsigned)s * 128u, sb = stage_addr(st);
+        // the start address is the descriptor's low field: a K step of
+        // 4096 B adds 256
+        const unsigned long long ah = umma_desc(sA, 2048, 128);
+        const unsigned long long al = umma_desc(sA + ubytes, 2048, 128);
+        const unsigned long long bh = umma_desc(sb, 2048, 128);
+        const unsigned long long bl = umma_desc(sb + ubytes, 2048, 128);
         for (int ks = 0; ks < U / 2; ks++) {
-          const unsigned off = (unsigned)ks * 4096u;
-          const unsigned long long ah = umma_desc(sA + off, 2048, 128);
-          const unsigned long long al = umma_desc(sA + ubytes + off, 2048, 128);
-          const unsigned long long bh = umma_desc(sb + off, 2048, 128);
-          const unsigned long long bl = umma_desc(sb + ubytes + off, 2048, 128);
-          umma_tf32(dt, ah, bh, idesc, ks > 0 ? 1u : 0u);
-          umma_tf32(dt, ah, bl, idesc, 1u);
-          umma_tf32(dt, al, bh, idesc, 1u);
+          const unsigned long long o = (unsigned long long)ks * 256u;
+          umma_tf32(dt, ah + o, bh + o, idesc, ks > 0 ? 1u : 0u);
+          umma_tf32(dt, ah + o, bl + o, idesc, 1u);
+          umma_tf32(dt, al + o, bh + o, idesc, 1u);
         }
         umma_commit(barM[s]);
         mpend[s] = true;
@@ -457,15 +468,20 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
           tmem_ld32(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)s * 128u + (unsigned)c0,
                     v);
           const int j0 = pt * KNN_TC_M + c0;
+          // admission: -2 v < thr, i.e. v > -thr/2 (exact in FP32); the
+          // query itself is admitted too and dropped at the re-rank
+          const float m = L.mthr;
+          bool any = false;
 #pragma unroll
-          for (int h = 0; h < 32; h++) {
-            const int jj = j0 + h;
-            const float dd = -2.f * v[h];
-            if (knn_less(dd, jj, L.thr, L.thi) && jj != q && jj < n) {
-              qd[qc] = dd;
-              qi[qc] = jj;
-              qc++;
-            }
+          for (int h = 0; h < 32; h++) any |= v[h] > m;
+          if (any) {
+#pragma unroll
+            for (int h = 0; h < 32; h++)
+              if (v[h] > m) {
+                qd[qc] = -2.f * v[h];
+                qi[qc] = j0 + h;
+                qc++;
+              }
           }
           if (__any_sync(0xffffffffu, qc > KNN_TC_QMAX - 32)) {
 #pragma unroll 1
@@ -495,12 +511,17 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
   } else if (q < n) {
     // exact re-rank with the arithmetic of k_knn, then a sort by (distance,
     // index); unused slots keep (inf, INT_MAX) and sort last
+    // a list that never filled holds every candidate
     const float tail = L.thr;
-    const int full = n - 1 > KNN_TC_CAP;
+    const bool full = L.thr != INFINITY;
     const float *xq = X + (long)q * dim;
 #pragma unroll
     for (int e = 0; e < KNN_TC_CAP; e++) {
-      if (L.j[e] == 0x7fffffff) continue;
+      if (L.j[e] >= n || L.j[e] == q) {  // empty slot, padding row or the query itself
+        L.d[e] = INFINITY;
+        L.j[e] = 0x7fffffff;
+        continue;
+      }
       const float *xc = X + (long)L.j[e] * dim;
       float a = 0.f;
       for (int kk = 0; kk < dim; kk++) {
