@@ -5,7 +5,7 @@
 // Usage: sg_tsne_cuda [-d D] [-a alpha] [-m max_iter] [-e early_iter] [-h h]
 //                     [-p np] [-u perplexity] [-f err] [-g ng] [-s sim]
 //                     [-n points] [-t coo|hybrid|csr|2|3|0] [-l lambda]
-//                     [-G fixed|h] [-k kNN-file-is-P: 0|1] FILE
+//                     [-G fixed|h] [-k kNN-file-is-P: 0|1] [-b 0|1] FILE
 // FILE holds either a sparse stochastic matrix in Matrix Market coordinate
 // format (1-based "row col value", as buildPFromMTX, CU/utils.cu:335-409) or
 // dense points ("n d" then n*d values, as readXfromMTX, CU/utils.cu:216-256;
@@ -17,7 +17,9 @@
 // Initial coordinates come from yin2m.txt in the working directory when it
 // exists (as the reference's demo), else 1e-4 N(0,1).
 // Outputs: sgtsneEmbedding.txt (one point per line, as extractEmbeddingTextT)
-// and timeInfo.txt (appended, as ExtractTimeInfo).
+// and timeInfo.txt (appended, as ExtractTimeInfo); with -b 1 also
+// embedding.bin, the n*d FP32 coordinates dimension-major as the reference's
+// sgtsneCUDA returns them, written raw as extractEmbedding (CU/utils.cu:140-148).
 #include "sgtsne_b200.h"
 
 #include <cuda_runtime.h>
@@ -151,10 +153,10 @@ int main(int argc, char **argv) {
   sgt_params p;
   sgt_params_default(&p);
   float u = 30;
-  int mtx_mode = -1;
+  int mtx_mode = -1, write_bin = 0;
   opterr = 0;
   int opt;
-  while ((opt = getopt(argc, argv, "d:a:m:e:h:p:u:f:g:s:n:t:l:G:k:")) != -1) {
+  while ((opt = getopt(argc, argv, "d:a:m:e:h:p:u:f:g:s:n:t:l:G:k:b:")) != -1) {
     switch (opt) {
       case 'd': p.d = atoi(optarg); break;
       case 'm': p.max_iter = atoi(optarg); break;
@@ -179,6 +181,7 @@ int main(int argc, char **argv) {
       }
       case 'G': p.grid_mode = !strcmp(optarg, "fixed") ? SGT_GRID_FIXED : SGT_GRID_H; break;
       case 'k': mtx_mode = atoi(optarg); break;
+      case 'b': write_bin = atoi(optarg); break;
       case '?': std::cerr << "Unknown option: '" << char(optopt) << "'!" << std::endl; break;
     }
   }
@@ -262,6 +265,16 @@ int main(int argc, char **argv) {
       for (int j = 0; j < p.d; j++) f << y[i + (size_t)j * n] << " ";
       f << "\n";
     }
+  }
+  if (write_bin) {
+    FILE *fb = fopen("embedding.bin", "wb");
+    if (!fb || fwrite(y.data(), sizeof(float), (size_t)n * p.d, fb) != (size_t)n * p.d) {
+      std::cerr << "cannot write embedding.bin" << std::endl;
+      if (fb) fclose(fb);
+      sgt_destroy(ctx);
+      return 3;
+    }
+    fclose(fb);
   }
   {
     // appended in the layout of ExtractTimeInfo (CU/utils.cu:72-92); the

@@ -636,12 +636,16 @@ def test_cli_dense_and_mtx(torch, ctx, oracle, tmp_path):
         f.write(f"{n} {dim}\n")
         np.savetxt(f, X, fmt="%.7g")
     args = [exe, "-d", "2", "-m", "300", "-e", "100", "-u", str(u), "-t", "csr"]
-    r = subprocess.run(args + [str(tmp_path / "pts.txt")], cwd=tmp_path, capture_output=True,
-                       text=True, timeout=300)
+    r = subprocess.run(args + ["-b", "1", str(tmp_path / "pts.txt")], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     Y = np.loadtxt(tmp_path / "sgtsneEmbedding.txt")
     assert Y.shape == (n, 2) and np.isfinite(Y).all()
     assert np.abs(Y.mean(0)).max() < 1e-3
+    # embedding.bin: the same coordinates, raw FP32, dimension-major
+    Yb = np.fromfile(tmp_path / "embedding.bin", dtype=np.float32)
+    assert Yb.size == n * 2
+    assert np.allclose(Yb.reshape(2, n).T, Y, rtol=1e-5, atol=1e-6 * np.abs(Y).max())
     # the same stages from Python: kNN, max-normalised distances, perplexity
     nn = int(np.ceil(3 * u))
     idx = torch.empty(n * nn, dtype=torch.int32, device="cuda")
