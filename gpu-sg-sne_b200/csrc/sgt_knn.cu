@@ -346,10 +346,13 @@ struct TcList {
   }
 };
 
-__global__ void __launch_bounds__(KNN_TC_M, 1)
+// One CTA holds QB (1 or 2) blocks of 128 queries: warps 4a..4a+3 own query
+// block a, whose two accumulators sit at tensor-memory columns 256a and
+// 256a + 128; every candidate tile streamed in serves all of them.
+__global__ void __launch_bounds__(2 * KNN_TC_M, 1)
 k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
          const float *__restrict__ nrm, const unsigned *__restrict__ nmax,
-         const float *__restrict__ X, int n, int dim, int U, int nstage, int k,
+         const float *__restrict__ X, int n, int dim, int U, int QB, int nstage, int k,
          int *__restrict__ idx, float *__restrict__ d2,
          int *__restrict__ redo, int *__restrict__ nredo, int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -357,8 +360,12 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
   __shared__ unsigned tslot;
   __shared__ volatile int abort_flag;
   const int t = threadIdx.x, warp = t >> 5;
-  const int qb = blockIdx.x, q = qb * KNN_TC_M + t;
   const int nt = (n + KNN_TC_M - 1) / KNN_TC_M;
+  const int qb0 = blockIdx.x * QB;           // first query block of the CTA
+  const int na = min(QB, nt - qb0);          // query blocks that exist
+  const int qa = warp >> 2;                  // this warp's query block
+  const int q = (qb0 + qa) * KNN_TC_M + (t & (KNN_TC_M - 1));
+  const unsigned tcols = 256u * (unsigned)QB;
   const unsigned ubytes = (unsigned)U * 2048u, pbytes = 2u * ubytes;
   const unsigned sA = smem_u32(smem);
   const unsigned barA = smem_u32(&bars[0]);
@@ -372,8 +379,8 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;"
-                 ::"r"(smem_u32(&tslot)));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(&tslot)), "r"(tcols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -384,7 +391,7 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
   // of the phase each completes.  Tile ti sits in stage ti % nstage.
   bool cpend[3] = {false, false, false}, mpend[2] = {false, false};
   unsigned cpar[3] = {0, 0, 0}, mpar[2] = {0, 0};
-  auto stage_addr = [&](int st) { return sA + (unsigned)(st + 1) * pbytes; };
+  auto stage_addr = [&](int st) { return sA + (unsigned)(QB + st) * pbytes; };
   auto bar_full = [&](int st) { return smem_u32(&bars[1 + st]); };
   auto load_tile = [&](int ti) {
     const int st = ti % nstage;
@@ -394,8 +401,9 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
     cpar[st] = (unsigned)((ti / nstage) & 1);
   };
   if (t == 0) {
-    mbar_expect_tx(barA, pbytes);
-    bulk_g2s(sA, gA + (size_t)qb * pbytes, pbytes, barA);
+    mbar_expect_tx(barA, (unsigned)na * pbytes);
+    for (int a = 0; a < na; a++)
+      bulk_g2s(sA + (unsigned)a * pbytes, gA + (size_t)(qb0 + a) * pbytes, pbytes, barA);
     for (int ti = 0; ti < nstage && ti < nt; ti++) load_tile(ti);
   }
   // D = A B^T: M = 128, N = 128, FP32 accumulate, TF32 A and B, both K-major
@@ -423,18 +431,21 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
       if (ok) {
         cpend[st] = false;
         tc_fence_after();
-        const unsigned dt = tmem + (unsigned)s * 128u, sb = stage_addr(st);
+        const unsigned sb = stage_addr(st);
         // the start address is the descriptor's low field: a K step of
         // 4096 B adds 256
-        const unsigned long long ah = umma_desc(sA, 2048, 128);
-        const unsigned long long al = umma_desc(sA + ubytes, 2048, 128);
         const unsigned long long bh = umma_desc(sb, 2048, 128);
         const unsigned long long bl = umma_desc(sb + ubytes, 2048, 128);
-        for (int ks = 0; ks < U / 2; ks++) {
-          const unsigned long long o = (unsigned long long)ks * 256u;
-          umma_tf32(dt, ah + o, bh + o, idesc, ks > 0 ? 1u : 0u);
-          umma_tf32(dt, ah + o, bl + o, idesc, 1u);
-          umma_tf32(dt, al + o, bh + o, idesc, 1u);
+        for (int a = 0; a < na; a++) {
+          const unsigned dt = tmem + 256u * (unsigned)a + (unsigned)s * 128u;
+          const unsigned long long ah = umma_desc(sA + (unsigned)a * pbytes, 2048, 128);
+          const unsigned long long al = umma_desc(sA + (unsigned)a * pbytes + ubytes, 2048, 128);
+          for (int ks = 0; ks < U / 2; ks++) {
+            const unsigned long long o = (unsigned long long)ks * 256u;
+            umma_tf32(dt, ah + o, bh + o, idesc, ks > 0 ? 1u : 0u);
+            umma_tf32(dt, ah + o, bl + o, idesc, 1u);
+            umma_tf32(dt, al + o, bh + o, idesc, 1u);
+          }
         }
         umma_commit(barM[s]);
         mpend[s] = true;
@@ -461,11 +472,14 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
           // the MMAs of tile pt are done with their stage: refill it
           if (pt + nstage < nt) load_tile(pt + nstage);
         }
+      }
+      if (go && qa < na) {
 #pragma unroll 1
         for (int c0 = 0; c0 < 128; c0 += 32) {
           float v[32];
           __syncwarp();  // converged for the warp-wide tcgen05.ld
-          tmem_ld32(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)s * 128u + (unsigned)c0,
+          tmem_ld32(tmem + ((unsigned)((warp & 3) * 32) << 16) + 256u * (unsigned)qa +
+                        (unsigned)s * 128u + (unsigned)c0,
                     v);
           const int j0 = pt * KNN_TC_M + c0;
           // admission: -2 v < thr, i.e. v > -thr/2 (exact in FP32); the
@@ -569,7 +583,7 @@ k_knn_tc(const float4 *__restrict__ imgA, const float4 *__restrict__ imgB,
   __syncthreads();
   tc_fence_after();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
 }
 
 }  // namespace
@@ -596,11 +610,14 @@ static sgt_status knn_tc(sgt_ctx *ctx, int n, int dim, const float *X, int k, in
   const int nblk = (n + KNN_TC_M - 1) / KNN_TC_M;
   const size_t img_bytes = (size_t)nblk * 2 * U * 2048;
   const size_t pbytes = (size_t)2 * U * 2048;
-  // the query tile and two or three candidate stages; at least 120 KB so
-  // that one CTA runs per SM (its 256 tensor-memory columns are then never
-  // contended)
-  const int nstage = 4 * pbytes + 1024 <= 227 * 1024 ? 3 : 2;
-  const size_t smem = std::max<size_t>((1 + nstage) * pbytes, 120 * 1024);
+  // QB query tiles (two when they fit beside two candidate stages, so each
+  // candidate tile streamed in serves 256 queries) and two or three candidate
+  // stages; at least 120 KB so that one CTA runs per SM (its tensor-memory
+  // columns are then never contended)
+  const size_t smem_max = 227 * 1024 - 1024;
+  const int QB = 4 * pbytes <= smem_max ? 2 : 1;
+  const int nstage = (QB + 3) * pbytes <= smem_max ? 3 : 2;
+  const size_t smem = std::max<size_t>((QB + nstage) * pbytes, 120 * 1024);
   char *buf = nullptr;
   const size_t o_nrm = 2 * img_bytes, o_max = o_nrm + sizeof(float) * (size_t)nblk * KNN_TC_M;
   const size_t o_cnt = o_max + 16, o_redo = o_cnt + 16;
@@ -624,8 +641,8 @@ static sgt_status knn_tc(sgt_ctx *ctx, int n, int dim, const float *X, int k, in
     e = cudaFuncSetAttribute(k_knn_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
   if (e == cudaSuccess) {
-    k_knn_tc<<<nblk, KNN_TC_M, smem, s>>>(imgA, imgB, nrm, nmax, X, n, dim, U, nstage, k, idx,
-                                          d2, redo, cnt, cnt + 1);
+    k_knn_tc<<<(nblk + QB - 1) / QB, KNN_TC_M * QB, smem, s>>>(
+        imgA, imgB, nrm, nmax, X, n, dim, U, QB, nstage, k, idx, d2, redo, cnt, cnt + 1);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s);
