@@ -2,8 +2,11 @@
 // front of the perplexity equalisation (the reference's command line tool
 // calls FLANN, an approximate search, at
 // CU/testing_modules/demo_perplexity.cu:131; this search is exact).
+// Two methods return the same bits: the SIMT search (k_knn) and, for up to
+// 64 dimensions and 32 neighbours, a tensor-core filter (k_knn_tc, further
+// down) whose candidates are re-ranked with the SIMT search's arithmetic.
 //
-// One query per thread, 128 queries per CTA.  Candidates stream through
+// SIMT search: one query per thread, 128 queries per CTA.  Candidates stream through
 // shared memory in tiles of 64 points x 64 dimensions, queries in tiles of
 // 128 x 64; rows are padded to 68 floats so each thread's float4 loads of
 // its query and the (broadcast) float4 loads of a candidate are free of bank
