@@ -626,8 +626,10 @@ static sgt_status knn_tc(sgt_ctx *ctx, int n, int dim, const float *X, int k, in
   const size_t o_cnt = o_max + 16, o_redo = o_cnt + 16;
   const size_t total = o_redo + sizeof(int) * (size_t)n;
   cudaError_t e = cudaMallocAsync(&buf, total, s);
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // not sticky: clear it for the caller's next check
     return sgti_fail(ctx, SGT_ERR_NO_MEMORY, "sgt_knn: tensor-core operand images");
+  }
   float4 *imgA = reinterpret_cast<float4 *>(buf);
   float4 *imgB = reinterpret_cast<float4 *>(buf + img_bytes);
   float *nrm = reinterpret_cast<float *>(buf + o_nrm);
@@ -681,6 +683,10 @@ extern "C" sgt_status sgt_knn_ex(sgt_ctx *ctx, int n, int dim, const float *X, i
   sgt_status st;
   if (method == SGT_KNN_TENSOR || (method == SGT_KNN_AUTO && tc_ok && n >= 4096)) {
     st = knn_tc(ctx, n, dim, X, k, idx, d2, n_redo);
+    // the filter's operand images (about 16 bytes per point and dimension)
+    // did not fit: the automatic choice falls back to the SIMT search
+    if (st == SGT_ERR_NO_MEMORY && method == SGT_KNN_AUTO)
+      st = knn_simt(ctx, n, dim, X, k, nullptr, n, idx, d2);
   } else {
     st = knn_simt(ctx, n, dim, X, k, nullptr, n, idx, d2);
   }
