@@ -143,10 +143,18 @@ k_knn(const float *__restrict__ X, int n, int dim, int k, const int *__restrict_
 // core matrices of 8 rows x 16 bytes; unit u (4 dimensions) of all 128 rows
 // is 2 KB, so the leading-dimension offset (next 4 dimensions) is 2048 B and
 // the stride offset (next 8 rows) 128 B.  hi and lo images follow each
-// other.  A CTA holds its 128 queries' image and streams candidate images
-// through two or three stages by bulk copies; one thread issues the MMAs of
-// a 128 x 128 tile into one of two tensor-memory accumulators while the four
-// warps scan the other (tcgen05.ld, one query row per thread).
+// other.  A CTA holds the images of one or two blocks of 128 queries and
+// streams candidate images through two or three stages by bulk copies; one
+// thread issues the MMAs of each 128 x 128 tile into one of two
+// tensor-memory accumulators per query block while that block's four warps
+// scan the other (tcgen05.ld, one query row per thread).
+//
+// Descriptor fields follow the PTX ISA's tcgen05 shared-memory and
+// instruction descriptors (the same bit layout as CUTLASS's
+// cute::UMMA::SmemDescriptor and UMMA::InstrDescriptor): start address,
+// leading and stride byte offsets in 16-byte units, version 1 at bit 46,
+// no swizzle; D format F32 at bit 4, A and B formats TF32 (2) at bits 7 and
+// 10, both K-major, N/8 at bit 17 and M/16 at bit 24.
 constexpr int KNN_TC_M = 128;
 constexpr int KNN_TC_MAXK = 32;
 constexpr float KNN_TC_EPS = 1e-4f;
