@@ -350,7 +350,9 @@ sgt_status sgt_knn(sgt_ctx *ctx, int n, int dim, const float *X, int k, int *idx
      terms, FP32 accumulation) keep a list of 64 candidates per query,
      re-ranked with the SIMT arithmetic; queries whose list could miss a
      neighbour under the filter's error bound are redone by the SIMT search.
-   SGT_KNN_AUTO: the tensor-core filter where it applies and n >= 4096. */
+   SGT_KNN_AUTO: the tensor-core filter where it applies and n >= 4096,
+     the SIMT search otherwise or when the filter's operand images (about
+     16 bytes per point and dimension) do not fit in device memory. */
 enum { SGT_KNN_AUTO = 0, SGT_KNN_SIMT = 1, SGT_KNN_TENSOR = 2 };
 
 /* sgt_knn with a method; *n_redo (may be NULL) receives the number of
