@@ -191,7 +191,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
     if (clock64() - t0 > KNN_TC_SPIN) return false;
   }
 }
-// global -> shared bulk copy completing on an mbarrier (no multicast)
+// global -> shared bulk copy into this CTA's own shared memory, completing
+// on an mbarrier
 __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes,
                                          unsigned bar) {
   asm volatile(
