@@ -250,6 +250,36 @@ def run_params(S, args):
     return p
 
 
+def run_knn_compare(n, seed, ctx, dev):
+    """Both kNN methods on a bounded sample of the configuration's points
+    (the first n of a fresh draw): CUDA-synchronised wall times and whether
+    indices and distance bits agree.  A failure is reported, not raised."""
+    import torch
+
+    import sgtsne_b200 as S
+    from sgtsne_b200 import workloads as W
+    try:
+        X, _ = W.gmm_zipf(n, dim=50, ncomp=40, zipf_a=1.1, centre_var=25.0, seed=seed + 7)
+        Xd = torch.as_tensor(np.ascontiguousarray(X, np.float32), device=dev)
+        res = {}
+        for name, m in (("tensor", S.KNN_TENSOR), ("simt", S.KNN_SIMT)):
+            idx = torch.empty(n * 30, dtype=torch.int32, device=dev)
+            d2 = torch.empty(n * 30, dtype=torch.float32, device=dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            redo = ctx.knn(n, 50, Xd, 30, idx, d2, method=m)
+            res[name] = (time.perf_counter() - t0, idx.cpu().numpy(), d2.cpu().numpy(), redo)
+        del Xd
+        torch.cuda.empty_cache()
+        (tt, it, dt, redo), (ts, is_, ds, _) = res["tensor"], res["simt"]
+        return {"points": n, "dim": 50, "k": 30, "tensor_s": round(tt, 4), "simt_s": round(ts, 4),
+                "speedup": round(ts / tt, 2), "redone_by_simt": redo,
+                "identical": bool(np.array_equal(it, is_) and
+                                  np.array_equal(dt.view(np.uint32), ds.view(np.uint32)))}
+    except Exception as e:  # the comparison is informative only
+        return {"points": n, "error": f"{type(e).__name__}: {e}"}
+
+
 def run_ours(args, rank, world, local, dist):
     import torch
 
@@ -345,7 +375,9 @@ def run_ours(args, rank, world, local, dist):
     h2d = (srp.nbytes + sc.nbytes + sv.nbytes + Y0.nbytes) / (W + K)
     d2h = Y0.nbytes / (W + K)
 
-    batched = served = None
+    batched = served = knn_cmp = None
+    if rank == 0 and args.knn_compare > 0:
+        knn_cmp = run_knn_compare(args.knn_compare, args.seed, ctx, dev)
     if rank == 0 and args.batched:
         batched = run_batched_leg(args, ctx, stream, dev)
     if rank == 0 and args.served:
@@ -402,6 +434,7 @@ def run_ours(args, rank, world, local, dist):
                                 f"{W + K} iterations, D2H of Y"},
             "gpu_launches": launches,
             "clocks": clk,
+            "knn_compare": knn_cmp,
             "batched": batched,
             "served": served,
         }
@@ -546,6 +579,8 @@ def main():
     ap.add_argument("--no-expanded", dest="expanded", action="store_false",
                     help="skip the fixed expanded-state (largest grid) line")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
+    ap.add_argument("--knn-compare", type=int, default=200000,
+                    help="points of the tensor-core vs SIMT kNN comparison (0 = skip)")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched-embeddings line")
     ap.add_argument("--batch-jobs", type=int, default=64)
