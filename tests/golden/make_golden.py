@@ -85,4 +85,6 @@ def main(out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(REPO, "gpurun_out", "golden"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py OUTDIR")
+    main(sys.argv[1])
