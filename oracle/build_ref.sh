@@ -1,8 +1,8 @@
 #!/bin/bash
 # Compiles the reference's own CUDA sources, where they lie under
 # /root/reference, with the test-only harnesses of oracle/ref_harness into
-# oracle/_ref/ (git-ignored; the built .so files travel with the repository
-# to the GPU box).  Used only to produce golden vectors of the reference and
+# oracle/_ref/ (git-ignored; the built .so files are copied with the
+# working tree to the GPU machine).  Used only to produce golden vectors of the reference and
 # to time the reference's own GPU loop (oracle/ref_gpu_timing.py).
 set -e
 HERE="$(cd "$(dirname "$0")" && pwd)"

@@ -14,8 +14,8 @@ def pytest_configure(config):
 
 
 def pytest_collection_modifyitems(config, items):
-    # GPU tests run only where a device exists; on a CPU box they are skipped
-    # (the driver selects them explicitly with -m gpu on the GPU box).
+    # GPU tests run only where a CUDA device exists; elsewhere they are
+    # skipped (select them with -m gpu on a machine with a B200).
     try:
         import torch
         has_gpu = torch.cuda.is_available()

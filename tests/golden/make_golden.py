@@ -1,6 +1,6 @@
 """Generate golden vectors from the reference's own CUDA kernels.
 
-Run on a GPU box after `bash oracle/build_ref.sh` (which compiles the
+Run on a machine with a B200 after `bash oracle/build_ref.sh` (which compiles the
 reference sources in place into oracle/_ref/):
 
     python tests/golden/make_golden.py OUTDIR
