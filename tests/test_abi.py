@@ -36,6 +36,26 @@ def test_exports_every_declared_symbol(S):
     assert S.load().sgt_abi_version() == 1
 
 
+def header_arg_counts():
+    """Parameter count of every function prototype in the header."""
+    src = open(os.path.join(REPO, "include", "sgtsne_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(sgt_[a-z0-9_]+)\s*\(([^()]*)\)\s*;", src):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_header(S):
+    """Every ctypes signature takes as many arguments as the C prototype."""
+    counts = header_arg_counts()
+    assert len(counts) >= 25
+    for nm, (_, args) in S.SIGNATURES.items():
+        assert nm in counts, nm
+        assert len(args) == counts[nm], (nm, len(args), counts[nm])
+
+
 def test_no_device_is_reported_not_faked(S):
     try:
         import torch
