@@ -94,6 +94,22 @@ static sgt_status fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) {
   if (ctx) ctx->err = msg;
   return s;
 }
+// The status of the error bits a step leaves in SgtState::error: non-finite
+// coordinates first, then the capacity bits (outputs written, but not what
+// the reference computes).
+static sgt_status flag_status(sgt_ctx *ctx, int flags, int grid_points, const char *where) {
+  if (flags & SGT_EFLAG_NONFINITE)
+    return fail(ctx, SGT_ERR_NUMERIC, std::string(where) + ": non-finite coordinates");
+  if (flags & SGT_EFLAG_CHUNK_OVERFLOW)
+    return fail(ctx, SGT_ERR_CAPACITY,
+                std::string(where) + ": the S2G guard skipped points (charge grid incomplete)");
+  if (flags & SGT_EFLAG_GRID_CLAMP)
+    return fail(ctx, SGT_ERR_CAPACITY,
+                std::string(where) + ": the embedding needs a larger grid than provisioned; "
+                "the step ran on " + std::to_string(grid_points) +
+                " points per axis (raise max_grid)");
+  return SGT_OK;
+}
 cudaStream_t sgti_stream(sgt_ctx *ctx) { return ctx->stream; }
 int sgti_device(sgt_ctx *ctx) { return ctx->device; }
 sgt_status sgti_fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) { return fail(ctx, s, msg); }
@@ -170,6 +186,7 @@ const char *sgt_status_string(sgt_status s) {
     case SGT_ERR_UNSUPPORTED: return "unsupported";
     case SGT_ERR_NUMERIC: return "non-finite values";
     case SGT_ERR_NO_DEVICE: return "no CUDA device";
+    case SGT_ERR_CAPACITY: return "device capacity reached";
   }
   return "unknown";
 }
@@ -1186,6 +1203,15 @@ static sgt_status run_chunk(sgt_job *J, int iters) {
   return SGT_OK;
 }
 
+sgt_status sgt_job_prepare(sgt_job *J) {
+  if (!J) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  if (!J->gexec) CKS(instantiate(J, 1, &J->gexec));
+  if (!J->gexec_multi) CKS(instantiate(J, SGT_GRAPH_ITERS, &J->gexec_multi));
+  return SGT_OK;
+}
+
 sgt_status sgt_job_run(sgt_job *J, int iters) {
   if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
   sgt_ctx *ctx = J->ctx;
@@ -1358,12 +1384,11 @@ sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, in
   CK(cudaGetLastError());
   if (staging) {
     CK(cudaMemcpyAsync(y, staging, bytes, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
     CK(cudaFreeAsync(staging, s));
-  } else {
-    CK(cudaStreamSynchronize(s));
   }
-  return SGT_OK;
+  CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return flag_status(ctx, J->st_host->error, J->st_host->N, "sgt_job_get_y");
 }
 
 sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
@@ -1429,6 +1454,63 @@ static sgt_status profile_iteration(sgt_job *J, cudaStream_t s, cudaEvent_t *ev)
   CKS(enqueue_combine<D>(J, s));
   CK(cudaEventRecord(ev[6], s));
   return SGT_OK;
+}
+
+// Iterations stage by stage with per-iteration stage times in the layout of
+// the reference's timeInfo: slot 7 i + j of iteration i (counted from the
+// last sgt_job_set_y; only i < 1000, the reference's array holds 1000
+// iterations and puts its totals at 7000..7002).  j = 0 attractive term
+// (CU/gradient_descend.cu:72-75), 1 S2G, 2 G2G, 3 G2S (CU/nuconv.cu:71-104),
+// 4 forces and update (zetaAndForce, CU/Frep.cu:118-121; here the combine
+// kernel, which also applies dY, gains and momentum), 5 S2G..G2S (the nuconv
+// total, CU/Frep.cu:111-116), 6 preprocessing (min shift, charges, scaling;
+// here the centring, grid decision and binning sort, CU/Frep.cu:92-110).
+// Relayouts and KL records happen where sgt_job_run does them.
+extern "C" sgt_status sgt_job_run_timed(sgt_job *J, int iters, double *time_info) {
+  if (!J || iters < 0) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t ev[7] = {};
+  sgt_status st = SGT_OK;
+  for (int i = 0; i < 7 && st == SGT_OK; i++)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) st = fail(ctx, SGT_ERR_CUDA, "event create");
+  const int every = J->p.relayout_every, kl_every = J->p.kl_every;
+  for (int it = 0; it < iters && st == SGT_OK; it++) {
+    if (every > 0 && J->host_iter > 0 && J->host_iter % every == 0) {
+      st = relayout(J);
+      if (st != SGT_OK) break;
+    }
+    switch (J->d) {
+      case 1: st = profile_iteration<1>(J, s, ev); break;
+      case 2: st = profile_iteration<2>(J, s, ev); break;
+      default: st = profile_iteration<3>(J, s, ev); break;
+    }
+    if (st != SGT_OK) break;
+    cudaError_t e = cudaEventSynchronize(ev[6]);
+    if (e != cudaSuccess) {
+      st = fail(ctx, SGT_ERR_CUDA, std::string("sgt_job_run_timed: ") + cudaGetErrorString(e));
+      break;
+    }
+    const long gi = J->host_iter;
+    if (time_info && gi < 1000) {
+      // (from event, to event) per slot
+      static const int span[7][2] = {{4, 5}, {1, 2}, {2, 3}, {3, 4}, {5, 6}, {1, 4}, {0, 1}};
+      for (int j = 0; j < 7; j++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[span[j][0]], ev[span[j][1]]);
+        time_info[7 * gi + j] = ms;
+      }
+    }
+    J->host_iter++;
+    if (kl_every > 0 && (J->host_iter % kl_every) == 0) {
+      double kl = 0;
+      st = sgt_job_kl(J, -1.0, &kl);
+    }
+  }
+  for (int i = 0; i < 7; i++)
+    if (ev[i]) cudaEventDestroy(ev[i]);
+  return st;
 }
 
 extern "C" sgt_status sgt_job_profile(sgt_job *J, int iters, double *stage_ms) {
@@ -1502,9 +1584,7 @@ sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed, cons
   if (h_eff) *h_eff = J->st_host->h_eff;
   ctx->last_N = J->st_host->N;
   ctx->last_d = d;
-  if (J->st_host->error & SGT_EFLAG_NONFINITE)
-    return fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates");
-  return SGT_OK;
+  return flag_status(ctx, J->st_host->error, J->st_host->N, "sgt_repulsive");
 }
 
 sgt_status sgt_bins(sgt_ctx *ctx, int n, int d, float h, int ng_fixed, const float *y, int layout,
@@ -1866,19 +1946,22 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
     // against the exact sum (CU/gradient_descend.cu:203-213)
     for (int it = 0; it < p.max_iter && st == SGT_OK;) {
       if (it % 10 == 0) {
-        st = sgt_job_run(J, 1);
+        st = time_info ? sgt_job_run_timed(J, 1, time_info) : sgt_job_run(J, 1);
         double e = 0;
         if (st == SGT_OK) st = sgt_job_repulsive_error(J, &e);
         errs.push_back(e);
         it++;
       } else {
         const int k = std::min(10 - it % 10, p.max_iter - it);
-        st = sgt_job_run(J, k);
+        st = time_info ? sgt_job_run_timed(J, k, time_info) : sgt_job_run(J, k);
         it += k;
       }
     }
   } else if (st == SGT_OK) {
-    st = sgt_job_run(J, p.max_iter);
+    // with time_info, every iteration's stage times as the reference
+    // records them (stage by stage; the SpMV no longer overlaps the
+    // repulsion), else the captured graphs
+    st = time_info ? sgt_job_run_timed(J, p.max_iter, time_info) : sgt_job_run(J, p.max_iter);
   }
   if (st == SGT_OK) st = sgt_job_get_y(J, y_out, SGT_LAYOUT_DIM_MAJOR, 0, 1);
   const auto t2 = std::chrono::steady_clock::now();
@@ -1886,7 +1969,7 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
     // as the reference: [7000] the gradient descent (CU/gradient_descend.cu:
     // 247), [7001] the preparation of P (CU/sgtsne.cu:98), [7002] the whole
     // call (the demo's total, demo_perplexity.cu:201); the per-iteration
-    // stage times [7 i + j] are not recorded (iterations run as graphs)
+    // stage times [7 i + j] were written by sgt_job_run_timed
     time_info[7000] = std::chrono::duration<double, std::milli>(t2 - t1).count();
     time_info[7001] = std::chrono::duration<double, std::milli>(t1 - t0).count();
     time_info[7002] = std::chrono::duration<double, std::milli>(t2 - t0).count();
@@ -1894,8 +1977,7 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   if (st == SGT_OK) {
     sgt_job_info info;
     st = sgt_job_get_info(J, &info);
-    if (st == SGT_OK && (info.error_flags & SGT_EFLAG_NONFINITE))
-      st = fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates during the iterations");
+    if (st == SGT_OK) st = flag_status(ctx, info.error_flags, info.grid_points, "sgt_embed");
   }
   if (st == SGT_OK && p.compute_error > 0) {
     // appended to errorInfo.txt in the working directory, one line per run,
@@ -1926,6 +2008,7 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
 // until the process exits.  Limits: n <= SGT_NA_MAX_N points, d = 1 or 2,
 // grids up to 128 points per axis in 2-D (512 in 1-D).
 // ---------------------------------------------------------------------------
+#include <cuda.h>  // CUcontext / CUresult of the two driver entry points below
 #include <mutex>
 
 namespace {
@@ -1961,16 +2044,54 @@ static_assert(NA_BYTES < 8u << 20, "no-alloc scratch stays a few MB");
 // kernels receive the device address obtained with cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_sgt_noalloc_scratch[NA_BYTES];
 
+// The array's device address is looked up once per device and cached with
+// the identity of the CUDA context it was looked up in: after a
+// cudaDeviceReset the primary context is a new one, the old address is
+// stale, and the next call looks it up again.  The identity comes from the
+// driver's cuCtxGetCurrent / cuCtxGetId, reached through the runtime's
+// driver entry points (no link against libcuda); without them the address
+// is looked up on every call.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+
+static unsigned long long current_context_id() {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void *f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (PfnCtxGetCurrent)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (PfnCtxGetId)f;
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c) return 0;
+  if (get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
 static std::mutex g_na_mutex;
-static void *g_na_addr[64];  // device address of the scratch, per device
+static void *g_na_addr[64];                  // device address of the scratch, per device
+static unsigned long long g_na_ctx_id[64];   // context the address belongs to (0: none)
 
 static sgt_status noalloc_scratch(sgt_ctx *ctx, unsigned char **out) {
   std::lock_guard<std::mutex> lock(g_na_mutex);
   if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, SGT_ERR_UNSUPPORTED, "device index >= 64");
-  if (!g_na_addr[ctx->device]) {  // once per device, with that device current
+  // the device is current here (the caller set it), so its primary context
+  // is the current one
+  const unsigned long long id = current_context_id();
+  if (!g_na_addr[ctx->device] || id == 0 || g_na_ctx_id[ctx->device] != id) {
     void *p = nullptr;
     CK(cudaGetSymbolAddress(&p, g_sgt_noalloc_scratch));
     g_na_addr[ctx->device] = p;
+    g_na_ctx_id[ctx->device] = id;
   }
   *out = (unsigned char *)g_na_addr[ctx->device];
   return SGT_OK;
@@ -2053,8 +2174,7 @@ extern "C" sgt_status sgt_repulsive_noalloc(sgt_ctx *ctx, int n, int d, float h,
   if (zeta) *zeta = hs.Z;
   if (grid_points) *grid_points = hs.N;
   if (h_eff) *h_eff = hs.h_eff;
-  if (hs.error & SGT_EFLAG_NONFINITE) return fail(ctx, SGT_ERR_NUMERIC, "non-finite coordinates");
-  return SGT_OK;
+  return flag_status(ctx, hs.error, hs.N, "sgt_repulsive_noalloc");
 }
 
 // CSR -> ELL + COO on the device (the device twin of sgt_csr_to_hybrid)

@@ -29,7 +29,9 @@ KNN_AUTO, KNN_SIMT, KNN_TENSOR = 0, 1, 2
 LAYOUT_DIM_MAJOR, LAYOUT_POINT_MAJOR = 0, 1
 GRID_H, GRID_FIXED = 0, 1
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
-          4: "unsupported", 5: "non-finite values", 6: "no CUDA device"}
+          4: "unsupported", 5: "non-finite values", 6: "no CUDA device",
+          7: "device capacity reached"}
+ERR_CAPACITY = 7
 
 
 class SgtError(RuntimeError):
@@ -83,6 +85,8 @@ SIGNATURES = {
     "sgt_job_destroy": (None, [_vp]),
     "sgt_job_set_y": (_i, [_vp, _vp, _i, _i]),
     "sgt_job_run": (_i, [_vp, _i]),
+    "sgt_job_prepare": (_i, [_vp]),
+    "sgt_job_run_timed": (_i, [_vp, _i, _vp]),
     "sgt_job_get_y": (_i, [_vp, _vp, _i, _i, _i]),
     "sgt_job_get_info": (_i, [_vp, C.POINTER(JobInfo)]),
     "sgt_job_kl": (_i, [_vp, _d, C.POINTER(_d)]),
@@ -280,14 +284,23 @@ class Context:
         self.check(self.lib.sgt_csr_to_coo(self.h, n, nnz, _ptr(rowptr), _ptr(rows)), "csr_to_coo")
 
     # ---- library entry (host numpy arrays) ----
-    def embed(self, rowptr, col, val, params: Params, y_in=None):
+    def embed(self, rowptr, col, val, params: Params, y_in=None, y_out=None, time_info=None):
+        """sgt_embed on host arrays.  y_in / y_out: dim-major n*d (y_out, if
+        given, must be a C-contiguous float32 array of n*d values, e.g. a
+        view of pinned memory); time_info: None (no stage times; the
+        captured graphs run) or a float64 array of >= 7003 values.
+        Returns (Y point-major (n, d), time_info)."""
         n = len(rowptr) - 1
         rowptr = np.ascontiguousarray(rowptr, np.int32)
         col = np.ascontiguousarray(col, np.int32)
         val = np.ascontiguousarray(val, np.float32)
         yin = None if y_in is None else np.ascontiguousarray(y_in, np.float32)
-        y = np.empty(n * params.d, np.float32)
-        ti = np.zeros(7003, np.float64)
+        if y_out is None:
+            y = np.empty(n * params.d, np.float32)
+        else:
+            y = y_out
+            assert y.dtype == np.float32 and y.flags["C_CONTIGUOUS"] and y.size == n * params.d
+        ti = time_info  # None: NULL (the captured graphs, no stage times)
         self.check(self.lib.sgt_embed(self.h, n, _ptr(rowptr), _ptr(col), _ptr(val),
                                       C.byref(params), _ptr(yin), _ptr(y), _ptr(ti)), "embed")
         return y.reshape(params.d, n).T.copy(), ti
@@ -323,6 +336,17 @@ class Job:
 
     def run(self, iters):
         self.ctx.check(self.lib.sgt_job_run(self.h, int(iters)), "run")
+
+    def run_timed(self, iters, time_info=None):
+        """Iterations stage by stage; per-iteration stage ms in the
+        reference's timeInfo layout (time_info[7 i + j], i < 1000)."""
+        ti = time_info if time_info is not None else np.zeros(7003, np.float64)
+        self.ctx.check(self.lib.sgt_job_run_timed(self.h, int(iters), _ptr(ti)), "run_timed")
+        return ti
+
+    def prepare(self):
+        """Instantiate the iteration graphs now (sgt_job_prepare)."""
+        self.ctx.check(self.lib.sgt_job_prepare(self.h), "prepare")
 
     def get_y(self, out, layout, device_mem, centre=1):
         self.ctx.check(self.lib.sgt_job_get_y(self.h, _ptr(out), layout, int(device_mem),

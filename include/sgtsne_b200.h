@@ -29,7 +29,13 @@ typedef enum {
   SGT_ERR_NO_MEMORY = 3,   /* device or pinned allocation failed */
   SGT_ERR_UNSUPPORTED = 4, /* option outside what the engine implements */
   SGT_ERR_NUMERIC = 5,     /* non-finite coordinates detected */
-  SGT_ERR_NO_DEVICE = 6    /* no CUDA device */
+  SGT_ERR_NO_DEVICE = 6,   /* no CUDA device */
+  SGT_ERR_CAPACITY = 7     /* a device-side capacity was reached: the grid the
+                              embedding needs is larger than the one provisioned
+                              (max_grid; the step ran on the largest provisioned
+                              grid instead) or the S2G guard skipped points.
+                              The outputs are written but are not the ones the
+                              reference computes; sgt_last_error says which. */
 } sgt_status;
 
 /* Storage format of P for the attractive term: the values of the reference
@@ -112,9 +118,12 @@ const char *sgt_last_error(const sgt_ctx *ctx);
  * std::default_random_engine (CU/utils.cu:185-193).  y_out: host, dim-major
  * n*d, caller-owned (the reference returned a malloc'd array).
  * time_info: NULL or >= 7003 doubles; as the reference, [7000] = gradient
- * descent ms, [7001] = preparation of P ms, [7002] = whole call ms; the
- * per-iteration stage slots [7 i + j] are left as given (iterations run as
- * captured graphs; sgt_job_profile measures stages). */
+ * descent ms, [7001] = preparation of P ms, [7002] = whole call ms, and the
+ * stage times of iteration i < 1000 in [7 i + j] (the slots of
+ * sgt_job_run_timed).  Measuring them runs every iteration stage by stage
+ * on one stream, as the reference does, without the overlap of the
+ * attractive SpMV and the repulsion that the captured graphs have, so the
+ * iterations take longer.  NULL runs the captured graphs. */
 sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const int *col,
                      const float *val, const sgt_params *params,
                      const float *y_in, float *y_out, double *time_info);
@@ -132,8 +141,23 @@ sgt_status sgt_job_set_y(sgt_job *job, const float *y, int layout,
                          int mem_is_device);
 /* Queue `iters` iterations (captured CUDA graph); asynchronous. */
 sgt_status sgt_job_run(sgt_job *job, int iters);
+/* sgt_job_run stage by stage on one stream with CUDA events, writing the
+   stage times of iteration i (counted from the last sgt_job_set_y; i < 1000)
+   into time_info[7 i + j] in the layout of the reference's timeInfo
+   (kl_minimization, CU/gradient_descend.cu:53-101, 208-247; CU/Frep.cu:
+   81-125; CU/nuconv.cu:37-112): j = 0 attractive term, 1 S2G, 2 G2G, 3 G2S,
+   4 forces and update, 5 S2G to G2S, 6 centring, grid decision and binning.
+   Synchronises once per iteration; time_info may be NULL. */
+sgt_status sgt_job_run_timed(sgt_job *job, int iters, double *time_info);
+/* Capture and instantiate the iteration graphs sgt_job_run launches (one
+   iteration, and 16 chained iterations) now instead of on first use, so
+   that later sgt_job_run calls only launch them.  Runs nothing on the GPU. */
+sgt_status sgt_job_prepare(sgt_job *job);
 /* Copy the current coordinates out (synchronises).  centre = 1 subtracts the
-   mean like the reference does after the last iteration. */
+   mean like the reference does after the last iteration.  Returns
+   SGT_ERR_CAPACITY (coordinates still written) when an iteration since the
+   last sgt_job_set_y ran on a clamped grid or skipped points in S2G, and
+   SGT_ERR_NUMERIC when coordinates became non-finite. */
 sgt_status sgt_job_get_y(sgt_job *job, float *y, int layout, int mem_is_device,
                          int centre);
 typedef struct {
@@ -255,7 +279,10 @@ sgt_status sgt_attractive(sgt_ctx *ctx, int format, int n, int d, long nnz,
    (CU/Frep.cu:81-125; h-driven grid as CU/Frep_varGrid.cu:79-107 and
    CU/gradient_descend_varGrid.cu:83-92).  ng_fixed > 0 forces the inner grid
    getBestGridSize(ng_fixed).  Outputs: f (normalised by Z, layout as y),
-   *zeta, *grid_points, *h_eff (host pointers, any may be NULL). */
+   *zeta, *grid_points, *h_eff (host pointers, any may be NULL).  An
+   embedding whose h-driven grid exceeds the largest this operator provisions
+   (512 points per axis for d <= 2, 128 for d = 3) is computed on that
+   largest grid and returns SGT_ERR_CAPACITY with the outputs written. */
 sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
                          const float *y, int layout, float *f, double *zeta,
                          int *grid_points, float *h_eff);
@@ -271,11 +298,15 @@ sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
    Limits: 2 <= n <= 32768, d = 1 or 2, a grid of at most 128 points per axis
    in 2-D (512 in 1-D); anything larger is rejected with SGT_ERR_INVALID_ARG
    and a message (an embedding wider than the limit is detected after the
-   work ran, its forces are not written to be used).
-   The first call on a device looks up the array's device address
-   (cudaGetSymbolAddress) and must come before any stream capture.  Calls
-   share the array: calls that overlap on the GPU (other streams, other host
-   threads on the same device) race and must be serialised by the caller. */
+   work ran, its forces are not written to be used).  Points skipped by the
+   S2G guard return SGT_ERR_CAPACITY, as in sgt_repulsive.
+   The first call on a device (and the first after that device's context
+   was reset) looks up the array's device address (cudaGetSymbolAddress) and
+   should come before any stream capture.  Every call waits for its work on
+   the context's stream to finish before it returns (it reads Z and the
+   grid back to the host).  Calls share the array: calls that overlap on the
+   GPU (other streams, other host threads on the same device) race and must
+   be serialised by the caller. */
 sgt_status sgt_repulsive_noalloc(sgt_ctx *ctx, int n, int d, float h,
                                  int ng_fixed, const float *y, int layout,
                                  float *f, double *zeta, int *grid_points,

@@ -2,14 +2,17 @@
 // (code/cuda/SG-tSNE-CUDA/src): AttractiveEstimation in COO format
 // (pq.cu:24-57) and computeFrepulsive_interp on the fixed grid
 // (Frep.cu:81-125, buffers and cuFFT plans set up as gradient_descend.cu:
-// 137-188 does), and the whole loop kl_minimization (gradient_descend.cu:
-// 102-282) for timing the reference's GPU path.  Compiled in place from the
-// reference tree by oracle/build_ref.sh; test and measurement use only.
+// 137-188 does), the whole loop kl_minimization (gradient_descend.cu:
+// 102-282; golden trajectories and timing of the reference's GPU path), the
+// cost tsneCost (pq.cu:104-125) and perplexityEqualization
+// (perplexity_search.cu:113-208).  Compiled in place from the reference tree
+// by oracle/build_ref.sh; test and measurement use only.
 #include <cmath>
 #include <cstring>
 #include <vector>
 #include "Frep.cuh"
 #include "gradient_descend.cuh"
+#include "perplexity_search.cuh"
 #include "pq.cuh"
 #include "types.hpp"
 
@@ -161,4 +164,71 @@ extern "C" double ref_cu_kl_minimization(int format, int n, int d, int nnz, int 
   Blocks = saved_blocks;
   Threads = saved_threads;
   return e == cudaSuccess ? ms : -(double)e;
+}
+
+// tsneCost on P in COO form (rows, cols, vals per nonzero) and dim-major y,
+// in FP32 (the reference's float instantiation) and FP64 (its double one).
+template <typename T>
+static T ref_cost(int n, int d, int nnz, const int *rows, const int *cols, const T *vals,
+                  const T *y_dim_major, T alpha, T zeta) {
+  int *dr, *dc;
+  T *dv, *dy;
+  cudaMallocManaged(&dr, sizeof(int) * (size_t)nnz);
+  cudaMallocManaged(&dc, sizeof(int) * (size_t)nnz);
+  cudaMallocManaged(&dv, sizeof(T) * (size_t)nnz);
+  cudaMallocManaged(&dy, sizeof(T) * (size_t)n * d);
+  cudaMemcpy(dr, rows, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice);
+  cudaMemcpy(dc, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice);
+  cudaMemcpy(dv, vals, sizeof(T) * (size_t)nnz, cudaMemcpyHostToDevice);
+  cudaMemcpy(dy, y_dim_major, sizeof(T) * (size_t)n * d, cudaMemcpyHostToDevice);
+  cudaDeviceSynchronize();
+  sparse_matrix<T> P;
+  memset(&P, 0, sizeof(P));
+  P.n = n;
+  P.m = n;
+  P.nnz = nnz;
+  P.format = 2;
+  P.row = dr;
+  P.col = dc;
+  P.val = dv;
+  const T c = tsneCost(P, dy, n, d, alpha, zeta);
+  cudaDeviceSynchronize();
+  cudaFree(dr); cudaFree(dc); cudaFree(dv); cudaFree(dy);
+  return c;
+}
+
+extern "C" float ref_cu_tsne_cost_f32(int n, int d, int nnz, const int *rows, const int *cols,
+                                      const float *vals, const float *y_dim_major, float alpha,
+                                      float zeta) {
+  return ref_cost<float>(n, d, nnz, rows, cols, vals, y_dim_major, alpha, zeta);
+}
+
+extern "C" double ref_cu_tsne_cost_f64(int n, int d, int nnz, const int *rows, const int *cols,
+                                       const double *vals, const double *y_dim_major,
+                                       double alpha, double zeta) {
+  return ref_cost<double>(n, d, nnz, rows, cols, vals, y_dim_major, alpha, zeta);
+}
+
+// perplexityEqualization: I and D are n x (nn + 1) (the point itself first,
+// at distance 0, as the reference's kNN search returns them); out_row
+// (n + 1), out_col and out_val (n * nn) receive the CSR it builds.  Returns
+// a CUDA error code.
+extern "C" int ref_cu_perplexity(int n, int nn, const int *I, const float *D, float u,
+                                 int *out_row, int *out_col, float *out_val) {
+  const size_t cnt = (size_t)n * (nn + 1);
+  int *dI;
+  float *dD;
+  cudaMallocManaged(&dI, sizeof(int) * cnt);
+  cudaMallocManaged(&dD, sizeof(float) * cnt);
+  cudaMemcpy(dI, I, sizeof(int) * cnt, cudaMemcpyHostToDevice);
+  cudaMemcpy(dD, D, sizeof(float) * cnt, cudaMemcpyHostToDevice);
+  cudaDeviceSynchronize();
+  sparse_matrix<float> P = perplexityEqualization(dI, dD, n, nn, u);
+  cudaError_t e = cudaDeviceSynchronize();
+  cudaMemcpy(out_row, P.row, sizeof(int) * (size_t)(n + 1), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_col, P.col, sizeof(int) * (size_t)n * nn, cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_val, P.val, sizeof(float) * (size_t)n * nn, cudaMemcpyDeviceToHost);
+  cudaFree(P.row); cudaFree(P.col); cudaFree(P.val);
+  cudaFree(dI); cudaFree(dD);
+  return (int)e;
 }

@@ -296,8 +296,14 @@ def test_embed_dropin(torch, ctx, oracle):
     Y0 = (np.random.default_rng(3).standard_normal((n, 2)) * 1e-2).astype(np.float32)
     p = S.default_params(d=2, lambda_=1.0, max_iter=300, early_iter=100, format=S.FORMAT_CSR)
     p.lambda_ = 10.0
-    Y, ti = ctx.embed(rp, col, val, p, y_in=Y0.T.copy())
+    Y, ti = ctx.embed(rp, col, val, p, y_in=Y0.T.copy(), time_info=np.zeros(7003))
     assert np.abs(Y.mean(0)).max() < 1e-3
+    # per-iteration stage times in the reference's timeInfo layout: every
+    # slot of the 300 iterations filled, nothing beyond them
+    st = ti[:7000].reshape(1000, 7)
+    assert (st[:300] > 0).all() and (st[300:] == 0).all()
+    # slot 5 (S2G..G2S) spans slots 1-3
+    assert (st[:300, 5] >= 0.99 * st[:300, 1:4].sum(1)).all()
     vo, _ = oracle.lambda_rescale(rp, val.astype(np.float64), 10.0, dist=True)
     srp, sc, sv = oracle.symmetrize(rp, col, vo, 1.0 / (2 * n))
     Yo = oracle.kl_minimization(srp, sc, sv, Y0.astype(np.float64), 300, early_iter=100,
@@ -746,6 +752,45 @@ def test_smallest_embeddings(torch, ctx, d):
                     val, device_mem=False)
         job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
         job.run(40)
-        Y = job.get_y(np.empty((n, d), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        Y = np.empty((n, d), np.float32)
+        try:
+            job.get_y(Y, S.LAYOUT_POINT_MAJOR, False, 1)
+        except S.SgtError as e:  # the clamp is reported; the coordinates are written
+            assert e.status == S.ERR_CAPACITY and "max_grid" in str(e)
         assert (job.info().error_flags & ~2) == 0 and np.isfinite(Y).all()
         job.close()
+
+
+def test_grid_clamp_is_a_status(torch, ctx):
+    """An embedding wider than the provisioned grid runs on the largest
+    provisioned grid and says so: the job API (sgt_job_get_y), sgt_repulsive
+    and sgt_embed return SGT_ERR_CAPACITY with the outputs written, never
+    SGT_OK."""
+    import sgtsne_b200 as S
+    n, d = 3000, 2
+    rp, col, val, _ = make_problem(n=n, k=10, seed=91)
+    rng = np.random.default_rng(91)
+    # spread 300 at h = 0.7 needs several hundred grid points per axis
+    Yw = (rng.standard_normal((n, d)) * 300).astype(np.float32)
+    p = S.default_params(d=d, format=S.FORMAT_CSR, max_grid=64)
+    job = S.Job(ctx, p, rp, col, val.astype(np.float32), device_mem=False)
+    job.set_y(Yw, S.LAYOUT_POINT_MAJOR, False)
+    job.run(1)
+    Y = np.full((n, d), np.nan, np.float32)
+    with pytest.raises(S.SgtError) as e:
+        job.get_y(Y, S.LAYOUT_POINT_MAJOR, False, 1)
+    assert e.value.status == S.ERR_CAPACITY and "max_grid" in str(e.value)
+    inf = job.info()
+    assert inf.error_flags & 2 and inf.grid_points <= 64 and np.isfinite(Y).all()
+    # set_y starts a new run: the flag is cleared with the state
+    job.set_y((Yw * 1e-3).astype(np.float32), S.LAYOUT_POINT_MAJOR, False)
+    job.run(1)
+    job.get_y(Y, S.LAYOUT_POINT_MAJOR, False, 1)
+    job.close()
+    # the operator: h = 0.01 over an extent of ~60 needs ~6000 points per axis
+    Yo = (rng.standard_normal((n, d)) * 10).astype(np.float32)
+    f = torch.full((n * d,), float("nan"), dtype=torch.float32, device="cuda")
+    with pytest.raises(S.SgtError) as e:
+        ctx.repulsive(n, d, 0.01, 0, dev(torch, Yo), S.LAYOUT_POINT_MAJOR, f)
+    assert e.value.status == S.ERR_CAPACITY
+    assert torch.isfinite(f).all()
