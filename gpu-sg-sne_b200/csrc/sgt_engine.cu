@@ -1787,9 +1787,15 @@ sgt_status sgt_kl(sgt_ctx *ctx, int n, int d, long nnz, const int *rowptr, const
 sgt_status sgt_lambda_bisect(sgt_ctx *ctx, int n, const int *rowptr, float *val, float lambda,
                              int dist, float *sigma) {
   if (!ctx || !rowptr || !val || n < 1) return SGT_ERR_INVALID_ARG;
+  if (dist < 0 || dist > 2)
+    return fail(ctx, SGT_ERR_INVALID_ARG, "sgt_lambda_bisect: dist must be 0, 1 or 2");
   CK(cudaSetDevice(ctx->device));
-  k_lambda_bisect<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, ctx->stream>>>(
-      n, rowptr, val, (double)lambda, 1e-5, 100, dist, sigma, nullptr);
+  if (dist == 2)
+    k_lambda_bisect_cu<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, ctx->stream>>>(
+        n, rowptr, val, lambda, sigma);
+  else
+    k_lambda_bisect<<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, ctx->stream>>>(
+        n, rowptr, val, (double)lambda, 1e-5, 100, dist, sigma, nullptr);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return SGT_OK;

@@ -54,6 +54,57 @@ k_lambda_bisect(int n, const int *__restrict__ rowptr, float *__restrict__ val,
   }
 }
 
+// The steps of the reference's GPU kernel (CU/graph_rescaling.cu:11-94), for
+// bit-level parity with it: FP32 sums of expf over the row's entries, lane
+// by lane with a stride of 32 and then a shuffle-down tree; the bracket
+// starts at [-1e3, 1e7] and its upper end never doubles; and the bisection
+// step of the evaluation that meets the tolerance is still applied, so the
+// row is normalised with the sigma one step past the one that met it (the
+// reference updates sigma before its loop test sees the flag).  Values are
+// used as given (the reference's GPU kernel has no -log transform).
+__device__ __forceinline__ float warp_sum_down_f(float v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+__global__ void __launch_bounds__(SGT_THREADS)
+k_lambda_bisect_cu(int n, const int *__restrict__ rowptr, float *__restrict__ val,
+                   float lambda, float *__restrict__ sigma_out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * blockDim.x / 32;
+  const float tol = 1e-5f;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < n; i += warps) {
+    const int s = rowptr[i], e = rowptr[i + 1];
+    float a = -1e3f, c = 1e7f, sigma = 1.0f;
+    bool found = false;
+    int iter = 0;
+    while (!found && iter < 100) {
+      float sum = 0.0f;
+      for (int t = s + lane; t < e; t += 32) sum += expf(-val[t] * sigma);
+      sum = warp_sum_down_f(sum);
+      const float diff = sum - lambda;
+      if (diff < tol && diff > -tol) found = true;
+      if (diff > 0) {
+        a = sigma;
+        sigma = c > 1e7f ? 2 * a : (float)(0.5 * (double)(a + c));
+      } else {
+        c = sigma;
+        sigma = (float)(0.5 * (double)(a + c));
+      }
+      iter++;
+    }
+    float sum = 0.0f;
+    for (int t = s + lane; t < e; t += 32) {
+      const float p = expf(-val[t] * sigma);
+      val[t] = p;
+      sum += p;
+    }
+    sum = warp_sum_down_f(sum);
+    for (int t = s + lane; t < e; t += 32) val[t] = val[t] / sum;
+    if (lane == 0 && sigma_out) sigma_out[i] = sigma;
+  }
+}
+
 // D: n*k squared distances to the k nearest neighbours (self excluded).
 // P: n*k output, each row sums to one.
 #define SGT_PERP_MAXK 256

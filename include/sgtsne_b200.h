@@ -80,7 +80,9 @@ typedef struct {
   int sim;          /* reference synthetic-data switch; ignored         */
   /* additions */
   int grid_mode;    /* sgt_grid_mode (default SGT_GRID_H)               */
-  int lambda_dist;  /* 1: P values are distances, 0: probabilities      */
+  int lambda_dist;  /* 1: P values are distances, 0: probabilities,
+                       2: distances with the reference GPU kernel's steps
+                       (see sgt_lambda_bisect)                          */
   int max_grid;     /* largest grid points per axis to provision
                        (0 = 512 for d <= 2, 128 for d = 3)              */
   int kl_every;     /* > 0: record the KL cost every kl_every iters     */
@@ -281,8 +283,10 @@ sgt_status sgt_attractive(sgt_ctx *ctx, int format, int n, int d, long nnz,
    getBestGridSize(ng_fixed).  Outputs: f (normalised by Z, layout as y),
    *zeta, *grid_points, *h_eff (host pointers, any may be NULL).  An
    embedding whose h-driven grid exceeds the largest this operator provisions
-   (512 points per axis for d <= 2, 128 for d = 3) is computed on that
-   largest grid and returns SGT_ERR_CAPACITY with the outputs written. */
+   is computed on that largest grid and returns SGT_ERR_CAPACITY with the
+   outputs written; for d <= 2 that is 512 points per axis, the end of the
+   reference's grid-size table (CU/utils.cu:197-207), so only d = 3 (128
+   points per axis) can reach it. */
 sgt_status sgt_repulsive(sgt_ctx *ctx, int n, int d, float h, int ng_fixed,
                          const float *y, int layout, float *f, double *zeta,
                          int *grid_points, float *h_eff);
@@ -332,10 +336,16 @@ sgt_status sgt_kl(sgt_ctx *ctx, int n, int d, long nnz, const int *rowptr,
                   const int *col, const float *val, const float *y, int layout,
                   double alpha, double zeta, double *kl);
 
-/* lambda rescaling, one warp per row, FP64 sums.  Replaces
-   lambdaRescalingGPU (CU/graph_rescaling.cu:96-107) with the semantics of
-   HYB/graph_rescaling.cpp:19-104 (dist != 0: values are distances).
-   val is rescaled in place; sigma (device, n) may be NULL. */
+/* lambda rescaling, one warp per row.  Replaces lambdaRescalingGPU
+   (CU/graph_rescaling.cu:96-107).  dist = 1: values are distances, dist = 0:
+   probabilities (-log p first); both with the semantics of the reference's
+   CPU path HYB/graph_rescaling.cpp:19-104 and FP64 row sums: sigma solves
+   sum_j exp(-sigma v_ij) = lambda to 1e-5.  dist = 2: distances with the
+   steps of the reference's GPU kernel (CU/graph_rescaling.cu:11-94), bit for
+   bit: FP32, and the row normalised with sigma one bisection step past the
+   one that met the tolerance (rows that meet it early in a wide bracket
+   then miss lambda).  val is rescaled in place; sigma (device, n) may be
+   NULL. */
 sgt_status sgt_lambda_bisect(sgt_ctx *ctx, int n, const int *rowptr,
                              float *val, float lambda, int dist, float *sigma);
 

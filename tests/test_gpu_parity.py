@@ -787,10 +787,12 @@ def test_grid_clamp_is_a_status(torch, ctx):
     job.run(1)
     job.get_y(Y, S.LAYOUT_POINT_MAJOR, False, 1)
     job.close()
-    # the operator: h = 0.01 over an extent of ~60 needs ~6000 points per axis
-    Yo = (rng.standard_normal((n, d)) * 10).astype(np.float32)
-    f = torch.full((n * d,), float("nan"), dtype=torch.float32, device="cuda")
+    # the operator in 3-D provisions 128 points per axis; h = 0.1 over an
+    # extent of ~60 asks for the table's largest, 512 (in 2-D that largest
+    # is provisioned, as the reference's grid-size table ends there)
+    Yo = (rng.standard_normal((n, 3)) * 10).astype(np.float32)
+    f = torch.full((n * 3,), float("nan"), dtype=torch.float32, device="cuda")
     with pytest.raises(S.SgtError) as e:
-        ctx.repulsive(n, d, 0.01, 0, dev(torch, Yo), S.LAYOUT_POINT_MAJOR, f)
-    assert e.value.status == S.ERR_CAPACITY
+        ctx.repulsive(n, 3, 0.1, 0, dev(torch, Yo), S.LAYOUT_POINT_MAJOR, f)
+    assert e.value.status == S.ERR_CAPACITY and "max_grid" in str(e.value)
     assert torch.isfinite(f).all()
