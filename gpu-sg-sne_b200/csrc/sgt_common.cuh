@@ -161,3 +161,4 @@ __device__ __forceinline__ int sgt_best_grid_size_dev(int ng) {
 #define SGT_EFLAG_NONFINITE 1
 #define SGT_EFLAG_GRID_CLAMP 2
 #define SGT_EFLAG_CHUNK_OVERFLOW 4
+#define SGT_EFLAG_COPY_TIMEOUT 8  // a bulk copy into shared memory did not complete

@@ -84,7 +84,10 @@ struct sgt_job {
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
   double last_kl = 0.0;
-  float tune_ms[4] = {0, 0, 0, 0};  // row kernel ms for G = 4, 8, 16, 32
+  // row kernel ms for G = 4, 8, 16, 32 with the stream read through L1
+  // ([0..3]) and staged by bulk copies ([4..7])
+  float tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int bulk = 0;  // 1: the attractive SpMV stages P by bulk copies (k_attr_rows_bulk)
 };
 
 // ---------------------------------------------------------------------------
@@ -100,6 +103,10 @@ static sgt_status fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) {
 static sgt_status flag_status(sgt_ctx *ctx, int flags, int grid_points, const char *where) {
   if (flags & SGT_EFLAG_NONFINITE)
     return fail(ctx, SGT_ERR_NUMERIC, std::string(where) + ": non-finite coordinates");
+  if (flags & SGT_EFLAG_COPY_TIMEOUT)
+    return fail(ctx, SGT_ERR_CUDA,
+                std::string(where) + ": a bulk copy into shared memory did not complete "
+                "within its wait limit");
   if (flags & SGT_EFLAG_CHUNK_OVERFLOW)
     return fail(ctx, SGT_ERR_CAPACITY,
                 std::string(where) + ": the S2G guard skipped points (charge grid incomplete)");
@@ -580,7 +587,11 @@ static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   const VT *Yc = (const VT *)J->Ynext;
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n);
+    if (J->bulk)
+      k_attr_rows_bulk<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr,
+                                                        n, J->st);
+    else
+      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals, Yc,
@@ -757,15 +768,20 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
 // fastest of G = 4, 8, 16, 32 is kept.
 // ---------------------------------------------------------------------------
 template <int D, int G>
-static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1) {
+static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1,
+                       bool bulk) {
   typedef typename Vec<D>::T VT;
   cudaStream_t s = J->ctx->stream;
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {  // the first launch warms caches
     cudaEventRecord(e0, s);
     const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY, (VT *)tF,
-                                                 J->n);
+    if (bulk)
+      k_attr_rows_bulk<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
+                                                        (VT *)tF, J->n, J->st);
+    else
+      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
+                                                   (VT *)tF, J->n);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -789,11 +805,13 @@ static sgt_status tune_group_d(sgt_job *J) {
   const float *tY = buf;  // zero coordinates: the gather pattern of P, finite values
   float *tF = buf + np;
   const int cand[4] = {4, 8, 16, 32};
-  float t[4];
-  t[0] = time_spmv<D, 4>(J, tY, tF, e0, e1);
-  t[1] = time_spmv<D, 8>(J, tY, tF, e0, e1);
-  t[2] = time_spmv<D, 16>(J, tY, tF, e0, e1);
-  t[3] = time_spmv<D, 32>(J, tY, tF, e0, e1);
+  float t[8];
+  for (int b = 0; b < 2; b++) {
+    t[4 * b + 0] = time_spmv<D, 4>(J, tY, tF, e0, e1, b == 1);
+    t[4 * b + 1] = time_spmv<D, 8>(J, tY, tF, e0, e1, b == 1);
+    t[4 * b + 2] = time_spmv<D, 16>(J, tY, tF, e0, e1, b == 1);
+    t[4 * b + 3] = time_spmv<D, 32>(J, tY, tF, e0, e1, b == 1);
+  }
   cudaError_t e = cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -801,10 +819,14 @@ static sgt_status tune_group_d(sgt_job *J) {
   CK(e);
   CK(cudaGetLastError());
   int best = 0;
-  for (int k = 1; k < 4; k++)
+  for (int k = 1; k < 8; k++)
     if (t[k] < t[best]) best = k;
-  J->G = cand[best];
-  for (int k = 0; k < 4; k++) J->tune_ms[k] = t[k];
+  J->G = cand[best % 4];
+  J->bulk = best >= 4;
+  for (int k = 0; k < 8; k++) J->tune_ms[k] = t[k];
+  // the bulk variant reports a copy that did not complete through the
+  // job's error flags; timing runs leave none behind
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
   return SGT_OK;
 }
 
@@ -1140,6 +1162,12 @@ static bool is_attractive_kernel(const void *f) {
       (const void *)k_attr_rows<2, 16>, (const void *)k_attr_rows<2, 32>,
       (const void *)k_attr_rows<3, 4>, (const void *)k_attr_rows<3, 8>,
       (const void *)k_attr_rows<3, 16>, (const void *)k_attr_rows<3, 32>,
+      (const void *)k_attr_rows_bulk<1, 4>, (const void *)k_attr_rows_bulk<1, 8>,
+      (const void *)k_attr_rows_bulk<1, 16>, (const void *)k_attr_rows_bulk<1, 32>,
+      (const void *)k_attr_rows_bulk<2, 4>, (const void *)k_attr_rows_bulk<2, 8>,
+      (const void *)k_attr_rows_bulk<2, 16>, (const void *)k_attr_rows_bulk<2, 32>,
+      (const void *)k_attr_rows_bulk<3, 4>, (const void *)k_attr_rows_bulk<3, 8>,
+      (const void *)k_attr_rows_bulk<3, 16>, (const void *)k_attr_rows_bulk<3, 32>,
       (const void *)k_attr_ell<1>, (const void *)k_attr_ell<2>, (const void *)k_attr_ell<3>,
       (const void *)k_attr_coo<1>, (const void *)k_attr_coo<2>, (const void *)k_attr_coo<3>};
   for (const void *g : fs)
@@ -1405,7 +1433,8 @@ sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
   info->error_flags = J->st_host->error;
   info->nnz = J->nnz;
   info->row_group = J->G;
-  for (int k = 0; k < 4; k++) info->tune_ms[k] = J->tune_ms[k];
+  info->row_kernel = J->bulk;
+  for (int k = 0; k < 8; k++) info->tune_ms[k] = J->tune_ms[k];
   return SGT_OK;
 }
 

@@ -19,6 +19,7 @@
 // are sorted by distance, ties by index.
 #include "../../include/sgtsne_b200.h"
 #include "sgt_internal.h"
+#include "sgt_async.cuh"
 
 #include <algorithm>
 #include <string>
@@ -158,47 +159,11 @@ k_knn(const float *__restrict__ X, int n, int dim, int k, const int *__restrict_
 constexpr int KNN_TC_M = 128;
 constexpr int KNN_TC_MAXK = 32;
 constexpr float KNN_TC_EPS = 1e-4f;
-constexpr long long KNN_TC_SPIN = 4000000000LL;  // clock cycles before a wait gives up
 
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
 __device__ __forceinline__ float tf32_rna(float x) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
-}
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-// bounded wait for the phase with the given parity; false when it gave up
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  const long long t0 = clock64();
-  while (true) {
-    unsigned done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (clock64() - t0 > KNN_TC_SPIN) return false;
-  }
-}
-// global -> shared bulk copy into this CTA's own shared memory, completing
-// on an mbarrier
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes,
-                                         unsigned bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
 }
 // shared-memory matrix descriptor: K-major, no swizzle
 __device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo,

@@ -168,10 +168,14 @@ typedef struct {
   float h_eff;       /* grid spacing of the last step             */
   double zeta;       /* Z of the last step                        */
   double kl;         /* last KL value recorded (kl_every > 0)     */
-  int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
+  int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow,
+                        8 a bulk copy did not complete in time    */
   long nnz;          /* nonzeros of P                             */
   int row_group;     /* lanes per row picked by the autotuner      */
-  float tune_ms[4];  /* row kernel ms measured for 4, 8, 16, 32 lanes */
+  int row_kernel;    /* 0: P streamed through L1, 1: P staged in shared
+                        memory by bulk copies (picked by the autotuner) */
+  float tune_ms[8];  /* row kernel ms measured for 4, 8, 16, 32 lanes,
+                        [0..3] streamed through L1, [4..7] staged      */
 } sgt_job_info;
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
