@@ -18,6 +18,10 @@
 #define SGT_MAX_GRID 512        // largest grid (points per axis) of the size table
 #define SGT_FFT_LINES 8         // lines per CTA in the FFT axis passes
 #define SGT_THREADS 256
+// index of a row-group lane count G in {4, 8, 16, 32}
+__host__ __device__ constexpr int sgt_group_index(int G) {
+  return G == 4 ? 0 : (G == 8 ? 1 : (G == 16 ? 2 : 3));
+}
 
 // Lagrange cubic weights on 4 nodes (CU/gridding.cuh:13-22,
 // HYB/gridding.cpp:29-39).  Node f+a gets w[a]; the point lies between
@@ -161,4 +165,3 @@ __device__ __forceinline__ int sgt_best_grid_size_dev(int ng) {
 #define SGT_EFLAG_NONFINITE 1
 #define SGT_EFLAG_GRID_CLAMP 2
 #define SGT_EFLAG_CHUNK_OVERFLOW 4
-#define SGT_EFLAG_COPY_TIMEOUT 8  // a bulk copy into shared memory did not complete

@@ -55,6 +55,12 @@ struct sgt_job {
   float *ell_vals = nullptr;
   int ell_w = 0;
   int *perm = nullptr;  // engine slot -> caller's point index (nullptr: identity)
+  // a shard of a row-split embedding (sgt_shard_*): its rows are points
+  // row0.. of the whole coordinate array Ygather, from which the SpMV
+  // gathers; nullptr / 0 for a whole embedding
+  float *Ygather = nullptr;
+  int row0 = 0;
+  int n_gather = 0;  // points the columns of P index (n for a whole embedding)
   // locality relabelling (CSR format): scratch allocated on first use
   int *rowptr_alt = nullptr, *perm_alt = nullptr, *rl_p = nullptr, *rl_iperm = nullptr,
       *rl_hist = nullptr, *rl_len = nullptr, *rl_bsum = nullptr;
@@ -84,10 +90,13 @@ struct sgt_job {
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
   double last_kl = 0.0;
-  // row kernel ms for G = 4, 8, 16, 32 with the stream read through L1
-  // ([0..3]) and staged by bulk copies ([4..7])
+  // row kernel ms for G = 4, 8, 16, 32 with one block per row tile
+  // ([0..3], k_attr_rows) and with persistent blocks walking per-SM
+  // stretches of rows ([4..7], k_attr_rows_sm)
   float tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int bulk = 0;  // 1: the attractive SpMV stages P by bulk copies (k_attr_rows_bulk)
+  int sm_rows = 0;             // 1: the attractive SpMV is k_attr_rows_sm
+  unsigned *sm_ctr = nullptr;  // its per-stretch tile counters (SGT_SM_SLOTS + 1)
+  int nb_rows_sm[4] = {0, 0, 0, 0};  // its persistent grid for G = 4, 8, 16, 32
 };
 
 // ---------------------------------------------------------------------------
@@ -103,10 +112,6 @@ static sgt_status fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) {
 static sgt_status flag_status(sgt_ctx *ctx, int flags, int grid_points, const char *where) {
   if (flags & SGT_EFLAG_NONFINITE)
     return fail(ctx, SGT_ERR_NUMERIC, std::string(where) + ": non-finite coordinates");
-  if (flags & SGT_EFLAG_COPY_TIMEOUT)
-    return fail(ctx, SGT_ERR_CUDA,
-                std::string(where) + ": a bulk copy into shared memory did not complete "
-                "within its wait limit");
   if (flags & SGT_EFLAG_CHUNK_OVERFLOW)
     return fail(ctx, SGT_ERR_CAPACITY,
                 std::string(where) + ": the S2G guard skipped points (charge grid incomplete)");
@@ -279,14 +284,16 @@ const char *sgt_last_error(const sgt_ctx *ctx) { return ctx ? ctx->err.c_str() :
 // ---------------------------------------------------------------------------
 // validation of a CSR structure (host copy)
 // ---------------------------------------------------------------------------
-static sgt_status check_csr(sgt_ctx *ctx, int n, const int *rowptr, const int *col) {
+static sgt_status check_csr(sgt_ctx *ctx, int n, const int *rowptr, const int *col,
+                           int ncols = -1) {
+  if (ncols < 0) ncols = n;
   if (rowptr[0] != 0) return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr[0] != 0");
   for (int i = 0; i < n; i++)
     if (rowptr[i + 1] < rowptr[i])
       return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr not monotone at row " + std::to_string(i));
   const long nnz = rowptr[n];
   for (long t = 0; t < nnz; t++)
-    if (col[t] < 0 || col[t] >= n)
+    if (col[t] < 0 || col[t] >= ncols)
       return fail(ctx, SGT_ERR_INVALID_ARG, "column out of range at nonzero " + std::to_string(t));
   return SGT_OK;
 }
@@ -543,10 +550,10 @@ static sgt_status enqueue_bin_count(sgt_job *J, cudaStream_t s) {
   return SGT_OK;
 }
 
-// The rest of the repulsion: tile offsets, sort, S2G, G2G, G2S and Z.
-// ev (optional): events recorded after the binning, S2G and G2G stages.
+// Tile offsets, sort and S2G: the charge grid of this job's points.
+// ev (optional): events recorded after the binning and S2G stages.
 template <int D>
-static sgt_status enqueue_repulsion_rest(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+static sgt_status enqueue_scatter_part(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   typedef typename Node<D>::T NT;
@@ -562,12 +569,31 @@ static sgt_status enqueue_repulsion_rest(sgt_job *J, cudaStream_t s, cudaEvent_t
     k_s2g<3, 8><<<J->nb_s2g8, SGT_THREADS, J->smem_s2g8, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
   k_s2g_cell<D><<<J->nb_s2gc, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
   if (ev) CK(cudaEventRecord(ev[2], s));
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+// G2G and G2S: potentials at this job's points and Z (the sum over them,
+// minus their count).  ev (optional): event recorded after G2G.
+template <int D>
+static sgt_status enqueue_gather_part(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+  sgt_ctx *ctx = J->ctx;
+  typedef typename Vec<D>::T VT;
+  typedef typename Node<D>::T NT;
   CKS(enqueue_g2g<D>(J, s));
   if (ev) CK(cudaEventRecord(ev[3], s));
   k_g2s<D><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi,
-                                             (VT *)J->Frep, J->part_z, n);
+                                             (VT *)J->Frep, J->part_z, J->n);
   CK(cudaGetLastError());
   return SGT_OK;
+}
+
+// The rest of the repulsion: tile offsets, sort, S2G, G2G, G2S and Z.
+// ev (optional): events recorded after the binning, S2G and G2G stages.
+template <int D>
+static sgt_status enqueue_repulsion_rest(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+  CKS(enqueue_scatter_part<D>(J, s, ev));
+  return enqueue_gather_part<D>(J, s, ev);
 }
 
 template <int D>
@@ -584,14 +610,15 @@ static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   const int n = J->n;
-  const VT *Yc = (const VT *)J->Ynext;
+  const VT *Yc = (const VT *)(J->Ygather ? J->Ygather : J->Ynext);
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (J->bulk)
-      k_attr_rows_bulk<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr,
-                                                        n, J->st);
+    if (J->sm_rows)
+      k_attr_rows_sm<D, G><<<J->nb_rows_sm[sgt_group_index(G)], SGT_THREADS, 0, s>>>(
+          J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n, J->row0, J->sm_ctr);
     else
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n);
+      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
+                                                   J->row0);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals, Yc,
@@ -769,19 +796,19 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
 // ---------------------------------------------------------------------------
 template <int D, int G>
 static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1,
-                       bool bulk) {
+                       bool sm) {
   typedef typename Vec<D>::T VT;
   cudaStream_t s = J->ctx->stream;
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {  // the first launch warms caches
     cudaEventRecord(e0, s);
     const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (bulk)
-      k_attr_rows_bulk<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
-                                                        (VT *)tF, J->n, J->st);
+    if (sm)
+      k_attr_rows_sm<D, G><<<J->nb_rows_sm[sgt_group_index(G)], SGT_THREADS, 0, s>>>(
+          J->rowptr, J->pairs, (const VT *)tY, (VT *)tF, J->n, J->row0, J->sm_ctr);
     else
       k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
-                                                   (VT *)tF, J->n);
+                                                   (VT *)tF, J->n, J->row0);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -795,13 +822,27 @@ template <int D>
 static sgt_status tune_group_d(sgt_job *J) {
   sgt_ctx *ctx = J->ctx;
   cudaStream_t s = ctx->stream;
-  const size_t np = (size_t)J->n * J->S;
+  // coordinates for every point P's columns index, forces for its rows
+  const size_t np = (size_t)std::max(J->n, J->n_gather) * J->S;
   float *buf = nullptr;
   CK(cudaMallocAsync(&buf, sizeof(float) * np * 2, s));
   CK(cudaMemsetAsync(buf, 0, sizeof(float) * np * 2, s));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
+  CKS(jalloc(J, &J->sm_ctr, (size_t)SGT_SM_SLOTS + 1));
+  CK(cudaMemsetAsync(J->sm_ctr, 0, sizeof(unsigned) * (SGT_SM_SLOTS + 1), s));
+  {  // persistent grids of k_attr_rows_sm: every block resident at once
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 4>, SGT_THREADS, 0));
+    J->nb_rows_sm[0] = grid_blocks(ctx->nsm, occ);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 8>, SGT_THREADS, 0));
+    J->nb_rows_sm[1] = grid_blocks(ctx->nsm, occ);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 16>, SGT_THREADS, 0));
+    J->nb_rows_sm[2] = grid_blocks(ctx->nsm, occ);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 32>, SGT_THREADS, 0));
+    J->nb_rows_sm[3] = grid_blocks(ctx->nsm, occ);
+  }
   const float *tY = buf;  // zero coordinates: the gather pattern of P, finite values
   float *tF = buf + np;
   const int cand[4] = {4, 8, 16, 32};
@@ -822,11 +863,8 @@ static sgt_status tune_group_d(sgt_job *J) {
   for (int k = 1; k < 8; k++)
     if (t[k] < t[best]) best = k;
   J->G = cand[best % 4];
-  J->bulk = best >= 4;
+  J->sm_rows = best >= 4;
   for (int k = 0; k < 8; k++) J->tune_ms[k] = t[k];
-  // the bulk variant reports a copy that did not complete through the
-  // job's error flags; timing runs leave none behind
-  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
   return SGT_OK;
 }
 
@@ -916,6 +954,10 @@ static sgt_status relayout(sgt_job *J) {
   }
 }
 
+static sgt_status job_create_impl(sgt_ctx *ctx, const sgt_params *params, int n, int ncols,
+                                  const int *rowptr, const int *col, const float *val,
+                                  int mem_is_device, sgt_job **out);
+
 extern "C" {
 
 // ---------------------------------------------------------------------------
@@ -923,6 +965,16 @@ extern "C" {
 // ---------------------------------------------------------------------------
 sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const int *rowptr,
                           const int *col, const float *val, int mem_is_device, sgt_job **out) {
+  return job_create_impl(ctx, params, n, n, rowptr, col, val, mem_is_device, out);
+}
+
+}  // extern "C"
+
+// ncols: points the columns of P index (n for a whole embedding; all points
+// for a shard, whose n rows are a stretch of them)
+static sgt_status job_create_impl(sgt_ctx *ctx, const sgt_params *params, int n, int ncols,
+                                  const int *rowptr, const int *col, const float *val,
+                                  int mem_is_device, sgt_job **out) {
   if (!ctx || !params || !rowptr || !col || !val || !out) return SGT_ERR_INVALID_ARG;
   if (n < 2) return fail(ctx, SGT_ERR_INVALID_ARG, "need at least 2 points");
   if (params->d < 1 || params->d > 3) return fail(ctx, SGT_ERR_UNSUPPORTED, "d must be 1, 2 or 3");
@@ -941,12 +993,12 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   }
   const long nnz = hrp[n];
   if (nnz <= 0) return fail(ctx, SGT_ERR_INVALID_ARG, "P has no nonzeros");
-  if (!mem_is_device) CKS(check_csr(ctx, n, hrp.data(), col));
+  if (!mem_is_device) CKS(check_csr(ctx, n, hrp.data(), col, ncols));
   if (mem_is_device) {
     int *bad = nullptr;
     CK(cudaMallocAsync(&bad, sizeof(int), s));
     CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
-    k_validate_csr<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(n, rowptr, col, bad);
+    k_validate_csr<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(n, ncols, rowptr, col, bad);
     int hb = 0;
     CK(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -960,6 +1012,7 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   J->n = n;
   J->d = params->d;
   J->nnz = nnz;
+  J->n_gather = ncols;
   J->format = params->format;
   J->G = choose_group(nnz, n);
   fill_jp(J);
@@ -1073,6 +1126,8 @@ sgt_status sgt_job_create(sgt_ctx *ctx, const sgt_params *params, int n, const i
   return SGT_OK;
 }
 
+extern "C" {
+
 void sgt_job_destroy(sgt_job *J) {
   if (!J) return;
   if (J->ctx) cudaSetDevice(J->ctx->device);
@@ -1162,12 +1217,12 @@ static bool is_attractive_kernel(const void *f) {
       (const void *)k_attr_rows<2, 16>, (const void *)k_attr_rows<2, 32>,
       (const void *)k_attr_rows<3, 4>, (const void *)k_attr_rows<3, 8>,
       (const void *)k_attr_rows<3, 16>, (const void *)k_attr_rows<3, 32>,
-      (const void *)k_attr_rows_bulk<1, 4>, (const void *)k_attr_rows_bulk<1, 8>,
-      (const void *)k_attr_rows_bulk<1, 16>, (const void *)k_attr_rows_bulk<1, 32>,
-      (const void *)k_attr_rows_bulk<2, 4>, (const void *)k_attr_rows_bulk<2, 8>,
-      (const void *)k_attr_rows_bulk<2, 16>, (const void *)k_attr_rows_bulk<2, 32>,
-      (const void *)k_attr_rows_bulk<3, 4>, (const void *)k_attr_rows_bulk<3, 8>,
-      (const void *)k_attr_rows_bulk<3, 16>, (const void *)k_attr_rows_bulk<3, 32>,
+      (const void *)k_attr_rows_sm<1, 4>, (const void *)k_attr_rows_sm<1, 8>,
+      (const void *)k_attr_rows_sm<1, 16>, (const void *)k_attr_rows_sm<1, 32>,
+      (const void *)k_attr_rows_sm<2, 4>, (const void *)k_attr_rows_sm<2, 8>,
+      (const void *)k_attr_rows_sm<2, 16>, (const void *)k_attr_rows_sm<2, 32>,
+      (const void *)k_attr_rows_sm<3, 4>, (const void *)k_attr_rows_sm<3, 8>,
+      (const void *)k_attr_rows_sm<3, 16>, (const void *)k_attr_rows_sm<3, 32>,
       (const void *)k_attr_ell<1>, (const void *)k_attr_ell<2>, (const void *)k_attr_ell<3>,
       (const void *)k_attr_coo<1>, (const void *)k_attr_coo<2>, (const void *)k_attr_coo<3>};
   for (const void *g : fs)
@@ -1356,6 +1411,239 @@ void sgt_batch_destroy(sgt_batch *b) {
   delete b;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// One embedding split by rows over ranks (sgt_shard_*).  A shard is a job
+// whose n rows are points row0 .. row0 + n - 1 of the whole embedding: P's
+// rows of those points (global column indices), their momentum, gains and
+// forces.  Three buffers belong to the caller and are exchanged between
+// ranks by the caller's collectives between the phases of an iteration:
+//   y_all  the coordinates of every point (stride S floats per point), the
+//          shard's own rows updated in place by the update phase;
+//   grid   the charge grid: S2G of the shard's own points, then the sum
+//          over ranks (grid_floats floats, all of which the caller reduces);
+//   zsum   one double: Z summed over the shard's own points, then over ranks.
+// ---------------------------------------------------------------------------
+struct sgt_shard {
+  sgt_job *J = nullptr;
+  int n_all = 0;       // points of the whole embedding
+  float *y_all = nullptr;
+  float *grid = nullptr;
+  size_t grid_floats = 0;
+  double *zsum = nullptr;
+  SgtJobParams jp_all{};  // the job's parameters with n = n_all (grid decision)
+};
+
+template <int D>
+static sgt_status shard_stats(sgt_shard *sh, cudaStream_t s) {
+  sgt_job *J = sh->J;
+  sgt_ctx *ctx = J->ctx;
+  // min, max and mean over every point: the grid decision all ranks share
+  k_init_stats<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const typename Vec<D>::T *)sh->y_all,
+                                                    sh->n_all, J->st, sh->jp_all, J->part_min,
+                                                    J->part_max, J->part_sum, 1);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+
+template <int D>
+static sgt_status shard_scatter_d(sgt_shard *sh) {
+  sgt_job *J = sh->J;
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  CKS(shard_stats<D>(sh, s));
+  // the attractive SpMV of the own rows on the side stream: it overlaps the
+  // grid reduction and the convolution, and the update phase joins it
+  CK(cudaEventRecord(J->ev_fork, s));
+  CK(cudaStreamWaitEvent(ctx->side, J->ev_fork, 0));
+  CKS(dispatch_attractive<D>(J, ctx->side));
+  CK(cudaEventRecord(J->ev_join, ctx->side));
+  // every float of the buffer is reduced: clear what this grid does not use
+  CK(cudaMemsetAsync(sh->grid, 0, sizeof(float) * sh->grid_floats, s));
+  CKS(enqueue_bin_count<D>(J, s));
+  return enqueue_scatter_part<D>(J, s);
+}
+
+template <int D>
+static sgt_status shard_update_d(sgt_shard *sh) {
+  sgt_job *J = sh->J;
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(&J->st->Z, sh->zsum, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CK(cudaStreamWaitEvent(s, J->ev_join, 0));
+  return enqueue_combine<D>(J, s);
+}
+
+extern "C" {
+
+size_t sgt_shard_grid_floats(const sgt_params *params) {
+  if (!params || params->d < 1 || params->d > 3) return 0;
+  const int D = params->d;
+  int max_grid = params->max_grid > 0 ? params->max_grid : (D <= 2 ? 512 : 128);
+  max_grid = std::min(D == 3 ? 256 : 512, std::max(16, max_grid));
+  int M = 1;
+  while (M < 2 * max_grid - 1) M <<= 1;
+  if (D == 1) M = std::max(M, 32);
+  const size_t nmax = std::min(512, (M + 1) / 2);
+  size_t nodes = nmax;
+  if (D >= 2) nodes *= nmax;
+  if (D >= 3) nodes *= nmax;
+  return nodes * (D == 1 ? 2 : 4);
+}
+
+sgt_status sgt_shard_create(sgt_ctx *ctx, const sgt_params *params, int n_all, int row0,
+                            int nrows, const int *rowptr, const int *col, const float *val,
+                            int mem_is_device, float *y_all, float *grid, size_t grid_floats,
+                            double *zsum, sgt_shard **out) {
+  if (!ctx || !params || !rowptr || !col || !val || !y_all || !grid || !zsum || !out)
+    return SGT_ERR_INVALID_ARG;
+  if (n_all < 2 || row0 < 0 || nrows < 1 || (long)row0 + nrows > n_all)
+    return fail(ctx, SGT_ERR_INVALID_ARG, "sgt_shard_create: rows outside [0, n_all)");
+  if (params->format != SGT_FORMAT_CSR)
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "sgt_shard_create: shards take P in CSR format");
+  if (params->relayout_every > 0 || params->kl_every > 0)
+    return fail(ctx, SGT_ERR_UNSUPPORTED, "sgt_shard_create: no relayout or in-loop KL");
+  sgt_job *J = nullptr;
+  CKS(job_create_impl(ctx, params, nrows, n_all, rowptr, col, val, mem_is_device, &J));
+  const size_t need = (size_t)J->nmax * (J->d >= 2 ? J->nmax : 1) * (J->d >= 3 ? J->nmax : 1) *
+                      (J->d == 1 ? 2 : 4);
+  if (grid_floats < need) {
+    sgt_job_destroy(J);
+    return fail(ctx, SGT_ERR_INVALID_ARG,
+                "sgt_shard_create: grid holds " + std::to_string(grid_floats) +
+                    " floats, the job's largest grid needs " + std::to_string(need));
+  }
+  sgt_shard *sh = new sgt_shard();
+  sh->J = J;
+  sh->n_all = n_all;
+  sh->y_all = y_all;
+  sh->grid = grid;
+  sh->grid_floats = grid_floats;
+  sh->zsum = zsum;
+  J->row0 = row0;
+  J->Ygather = y_all;
+  J->Ynext = y_all + (size_t)row0 * J->S;  // the own rows of the shared array
+  J->V = grid;
+  sh->jp_all = J->jp;
+  sh->jp_all.n = n_all;
+  *out = sh;
+  return SGT_OK;
+}
+
+void sgt_shard_destroy(sgt_shard *sh) {
+  if (!sh) return;
+  sgt_job_destroy(sh->J);
+  delete sh;
+}
+
+sgt_status sgt_shard_set_y(sgt_shard *sh, const float *y, int layout, int mem_is_device) {
+  if (!sh || !y) return SGT_ERR_INVALID_ARG;
+  sgt_job *J = sh->J;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t bytes = sizeof(float) * (size_t)sh->n_all * J->d;
+  const float *src = y;
+  float *staging = nullptr;
+  if (!mem_is_device) {
+    CK(cudaMallocAsync(&staging, bytes, s));
+    CK(cudaMemcpyAsync(staging, y, bytes, cudaMemcpyHostToDevice, s));
+    src = staging;
+  }
+  const int nb = grid_blocks(ctx->nsm, 4);
+  const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+  switch (J->d) {
+    case 1: k_pack<1><<<nb, SGT_THREADS, 0, s>>>(src, sh->n_all, dm, sh->y_all); break;
+    case 2: k_pack<2><<<nb, SGT_THREADS, 0, s>>>(src, sh->n_all, dm, (float2 *)sh->y_all); break;
+    default: k_pack<3><<<nb, SGT_THREADS, 0, s>>>(src, sh->n_all, dm, (float4 *)sh->y_all); break;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(J->uY, 0, sizeof(float) * (size_t)J->n * J->S, s));
+  k_fill<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(J->gains, (long)J->n * J->S, 1.0f);
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
+  CK(cudaMemsetAsync(J->tile_count, 0, sizeof(int) * SGT_HIST_MAX, s));
+  if (staging) CK(cudaFreeAsync(staging, s));
+  return SGT_OK;
+}
+
+sgt_status sgt_shard_scatter(sgt_shard *sh) {
+  if (!sh) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = sh->J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  switch (sh->J->d) {
+    case 1: return shard_scatter_d<1>(sh);
+    case 2: return shard_scatter_d<2>(sh);
+    default: return shard_scatter_d<3>(sh);
+  }
+}
+
+sgt_status sgt_shard_gather(sgt_shard *sh) {
+  if (!sh) return SGT_ERR_INVALID_ARG;
+  sgt_job *J = sh->J;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  switch (J->d) {
+    case 1: CKS(enqueue_gather_part<1>(J, s)); break;
+    case 2: CKS(enqueue_gather_part<2>(J, s)); break;
+    default: CKS(enqueue_gather_part<3>(J, s)); break;
+  }
+  CK(cudaMemcpyAsync(sh->zsum, &J->st->Z, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return SGT_OK;
+}
+
+sgt_status sgt_shard_update(sgt_shard *sh) {
+  if (!sh) return SGT_ERR_INVALID_ARG;
+  sgt_ctx *ctx = sh->J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  switch (sh->J->d) {
+    case 1: return shard_update_d<1>(sh);
+    case 2: return shard_update_d<2>(sh);
+    default: return shard_update_d<3>(sh);
+  }
+}
+
+sgt_status sgt_shard_get_y(sgt_shard *sh, float *y, int layout, int mem_is_device, int centre) {
+  if (!sh || !y) return SGT_ERR_INVALID_ARG;
+  sgt_job *J = sh->J;
+  sgt_ctx *ctx = J->ctx;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const size_t bytes = sizeof(float) * (size_t)sh->n_all * J->d;
+  float *dst = y, *staging = nullptr;
+  if (!mem_is_device) {
+    CK(cudaMallocAsync(&staging, bytes, s));
+    dst = staging;
+  }
+  // the mean over every point (the update phase leaves the own rows' one)
+  switch (J->d) {
+    case 1: CKS(shard_stats<1>(sh, s)); break;
+    case 2: CKS(shard_stats<2>(sh, s)); break;
+    default: CKS(shard_stats<3>(sh, s)); break;
+  }
+  const int nb = grid_blocks(ctx->nsm, 4);
+  const int dm = layout == SGT_LAYOUT_DIM_MAJOR;
+  switch (J->d) {
+    case 1: k_unpack_centred<1><<<nb, SGT_THREADS, 0, s>>>((const float *)sh->y_all, sh->n_all, dm, J->st, centre, nullptr, dst); break;
+    case 2: k_unpack_centred<2><<<nb, SGT_THREADS, 0, s>>>((const float2 *)sh->y_all, sh->n_all, dm, J->st, centre, nullptr, dst); break;
+    default: k_unpack_centred<3><<<nb, SGT_THREADS, 0, s>>>((const float4 *)sh->y_all, sh->n_all, dm, J->st, centre, nullptr, dst); break;
+  }
+  CK(cudaGetLastError());
+  if (staging) {
+    CK(cudaMemcpyAsync(y, staging, bytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaFreeAsync(staging, s));
+  }
+  CK(cudaMemcpyAsync(J->st_host, J->st, sizeof(SgtState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return flag_status(ctx, J->st_host->error, J->st_host->N, "sgt_shard_get_y");
+}
+
+sgt_status sgt_shard_get_info(sgt_shard *sh, sgt_job_info *info) {
+  if (!sh) return SGT_ERR_INVALID_ARG;
+  return sgt_job_get_info(sh->J, info);
+}
+
 // Device bytes of a job: the buffers of job_alloc, job_alloc_parts and P,
 // plus the largest transient of job creation (host P staged on the device,
 // or the autotuner's scratch copies).
@@ -1433,7 +1721,7 @@ sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
   info->error_flags = J->st_host->error;
   info->nnz = J->nnz;
   info->row_group = J->G;
-  info->row_kernel = J->bulk;
+  info->row_kernel = J->sm_rows;
   for (int k = 0; k < 8; k++) info->tune_ms[k] = J->tune_ms[k];
   return SGT_OK;
 }

@@ -190,8 +190,8 @@ __global__ void k_pack_pairs(long nnz, const int *__restrict__ col,
     pairs[e] = make_int2(col[e], __float_as_int(val[e]));
 }
 
-// flags a CSR whose rowptr decreases or whose columns leave [0, n)
-__global__ void k_validate_csr(int n, const int *__restrict__ rowptr,
+// flags a CSR whose rowptr decreases or whose columns leave [0, ncols)
+__global__ void k_validate_csr(int n, int ncols, const int *__restrict__ rowptr,
                                const int *__restrict__ col, int *__restrict__ bad) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int s = rowptr[i], e = rowptr[i + 1];
@@ -200,7 +200,7 @@ __global__ void k_validate_csr(int n, const int *__restrict__ rowptr,
       continue;
     }
     for (int t = s; t < e; t++)
-      if (col[t] < 0 || col[t] >= n) {
+      if (col[t] < 0 || col[t] >= ncols) {
         atomicOr(bad, 1);
         break;
       }

@@ -21,7 +21,6 @@
 // gains/momentum update and the reductions that decide the next iteration's
 // grid.  Y is double-buffered (the combine reads Y while writing Ynext).
 #pragma once
-#include "sgt_async.cuh"
 #include "sgt_common.cuh"
 #include "sgt_grid.cuh"
 
@@ -270,19 +269,21 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 // retire, so a long row delays one group, not a persistent warp).  Kept lean
 // (no loop state across rows) so 48+ warps stay resident per SM.  It reads
 // only Y and P, so the iteration runs it as a graph branch beside the
-// repulsion chain; k_row_update combines the two forces.
+// repulsion chain; k_row_update combines the two forces.  Row i is point
+// row0 + i of Y (a shard of a row-split embedding holds rows row0.. of P
+// with global column indices and gathers from the whole Y).
 // ---------------------------------------------------------------------------
 template <int D, int G>
 __global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
 k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
             const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
-            int n) {
+            int n, int row0) {
   const int lane = threadIdx.x % G;
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = i < n;
   float acc[3] = {0.f, 0.f, 0.f};
   if (valid) {
-    const typename Vec<D>::T yi = Y[i];
+    const typename Vec<D>::T yi = Y[row0 + i];
     csr_row_sum<D, G>(rowptr, pairs, Y, i, lane, yi, acc);
   }
   group_reduce<D, G>(acc);
@@ -296,83 +297,75 @@ k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 }
 
 // ---------------------------------------------------------------------------
-// The same SpMV with the block's stretch of P staged in shared memory by one
-// bulk copy (cp.async.bulk, the TMA engine).  The rows of a block own one
-// contiguous stretch of the (column, value) stream; copying it with the bulk
-// engine keeps the stream out of the L1TEX pipeline, which then serves only
-// the coordinate gathers, one 32-byte sector each (the stream adds another
-// quarter sector per nonzero when it is read through L1TEX).  A block whose
-// stretch exceeds the buffer reads it from global memory as k_attr_rows does.
-// The stream must be readable one pair past its end (jobs pad it by 8).
+// The same SpMV as a persistent kernel whose SMs each walk one contiguous
+// stretch of rows.  A block reads the id of the SM it runs on and takes row
+// tiles (SGT_THREADS / G rows) from that SM's stretch through one counter
+// per stretch, then from the stretches that follow once its own is done.
+// The blocks resident on one SM therefore work on neighbouring rows at any
+// time, and when the points are ordered for locality (relabelled) the
+// coordinates their rows gather stay in that SM's L1; k_attr_rows instead
+// spreads consecutive blocks over all SMs.  The last block to finish clears
+// the counters for the next launch.  ctr holds SGT_SM_SLOTS + 1 zeros.
 // ---------------------------------------------------------------------------
-#define SGT_ATTR_STAGE 2048  // pairs staged per block (16 KB)
+#define SGT_SM_SLOTS 512
 
 template <int D, int G>
 __global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
-k_attr_rows_bulk(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
-                 const typename Vec<D>::T *__restrict__ Y,
-                 typename Vec<D>::T *__restrict__ Fattr, int n, SgtState *__restrict__ st) {
+k_attr_rows_sm(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+               const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
+               int n, int row0, unsigned *__restrict__ ctr) {
   constexpr int RPB = SGT_THREADS / G;
-  __shared__ __align__(128) int2 sp[SGT_ATTR_STAGE];
-  __shared__ __align__(8) unsigned long long bar;
-  __shared__ int s_base, s_staged;
-  const int r0 = blockIdx.x * RPB;
-  if (r0 >= n) return;  // uniform over the block
-  const int r1 = min(r0 + RPB, n);
-  if (threadIdx.x == 0) {
-    const int s = rowptr[r0], e = rowptr[r1];
-    const int s0 = s & ~1;              // 16-byte aligned (pairs are 8 bytes)
-    const int cnt = (e - s0 + 1) & ~1;  // whole 16-byte units
-    const int staged = cnt > 0 && cnt <= SGT_ATTR_STAGE;
-    s_base = s0;
-    s_staged = staged;
-    if (staged) {
-      const unsigned b = smem_u32(&bar);
-      mbar_init(b, 1);
-      mbar_fence_init();
-      mbar_expect_tx(b, (unsigned)cnt * 8u);
-      bulk_g2s(smem_u32(sp), pairs + s0, (unsigned)cnt * 8u, b);
-    }
-  }
-  __syncthreads();
-  bool staged = s_staged != 0;
-  if (staged && !mbar_wait(smem_u32(&bar), 0)) {
-    // the copy did not complete in time: flag it and wait once more for the
-    // copy that may still be writing this block's shared memory; if it
-    // still has not landed, take the stream from global memory
-    atomicOr(&st->error, SGT_EFLAG_COPY_TIMEOUT);
-    staged = mbar_wait(smem_u32(&bar), 0);
-  }
+  __shared__ int s_tile;
+  unsigned smid, nsmid;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsmid));
+  const int ns = (int)min(max(nsmid, 1u), (unsigned)SGT_SM_SLOTS);
+  const int ntiles = (n + RPB - 1) / RPB;
+  int stretch = (int)(smid % (unsigned)ns), visited = 0;  // used by thread 0 only
   const int lane = threadIdx.x % G;
-  const int i = r0 + threadIdx.x / G;
-  const bool valid = i < r1;
-  float acc[3] = {0.f, 0.f, 0.f};
-  if (valid) {
-    const typename Vec<D>::T yi = Y[i];
-    const int s = rowptr[i], e = rowptr[i + 1];
-    constexpr int U = 4;
-    const int base = s_base;
-    for (int t0 = s + lane; t0 < e; t0 += U * G) {
-      int2 pr[U];
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int t = t0 + u * G;
-        pr[u] = t < e ? (staged ? sp[t - base] : __ldcs(&pairs[t])) : make_int2(i, 0);
+  while (true) {
+    if (threadIdx.x == 0) {
+      int tile = -1;
+      while (visited < ns) {
+        const int lo = (int)((long)stretch * ntiles / ns);
+        const int hi = (int)((long)(stretch + 1) * ntiles / ns);
+        const int k = lo < hi ? (int)atomicAdd(&ctr[stretch], 1u) : hi - lo;
+        if (k < hi - lo) {
+          tile = lo + k;
+          break;
+        }
+        stretch = stretch + 1 == ns ? 0 : stretch + 1;
+        visited++;
       }
-      typename Vec<D>::T yj[U];
+      s_tile = tile;
+    }
+    __syncthreads();
+    const int tile = s_tile;
+    __syncthreads();  // s_tile is written again in the next round
+    if (tile < 0) break;
+    const int i = tile * RPB + threadIdx.x / G;
+    const bool valid = i < n;
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (valid) {
+      const typename Vec<D>::T yi = Y[row0 + i];
+      csr_row_sum<D, G>(rowptr, pairs, Y, i, lane, yi, acc);
+    }
+    group_reduce<D, G>(acc);
+    if (valid && lane == 0) {
+      typename Vec<D>::T f;
+      if constexpr (D == 3) f.w = 0.f;
 #pragma unroll
-      for (int u = 0; u < U; u++) yj[u] = __ldg(&Y[pr[u].x]);
-#pragma unroll
-      for (int u = 0; u < U; u++) attr_term<D>(yi, yj[u], __int_as_float(pr[u].y), acc);
+      for (int k = 0; k < D; k++) setcomp<D>(f, k, acc[k]);
+      Fattr[i] = f;
     }
   }
-  group_reduce<D, G>(acc);
-  if (valid && lane == 0) {
-    typename Vec<D>::T f;
-    if constexpr (D == 3) f.w = 0.f;
-#pragma unroll
-    for (int k = 0; k < D; k++) setcomp<D>(f, k, acc[k]);
-    Fattr[i] = f;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctr[SGT_SM_SLOTS], 1u) == gridDim.x - 1) {
+      for (int k = 0; k < ns; k++) ctr[k] = 0u;
+      ctr[SGT_SM_SLOTS] = 0u;
+      __threadfence();
+    }
   }
 }
 

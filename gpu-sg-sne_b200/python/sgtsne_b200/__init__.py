@@ -125,6 +125,16 @@ SIGNATURES = {
     "sgt_knn_ex": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp, _i, C.POINTER(_i)]),
     "sgt_csr_to_hybrid_device": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp,
                                       C.POINTER(_l)]),
+    "sgt_shard_grid_floats": (C.c_size_t, [C.POINTER(Params)]),
+    "sgt_shard_create": (_i, [_vp, C.POINTER(Params), _i, _i, _i, _vp, _vp, _vp, _i, _vp, _vp,
+                              C.c_size_t, _vp, C.POINTER(_vp)]),
+    "sgt_shard_destroy": (None, [_vp]),
+    "sgt_shard_set_y": (_i, [_vp, _vp, _i, _i]),
+    "sgt_shard_scatter": (_i, [_vp]),
+    "sgt_shard_gather": (_i, [_vp]),
+    "sgt_shard_update": (_i, [_vp]),
+    "sgt_shard_get_y": (_i, [_vp, _vp, _i, _i, _i]),
+    "sgt_shard_get_info": (_i, [_vp, C.POINTER(JobInfo)]),
 }
 
 _LIB = None

@@ -168,14 +168,14 @@ typedef struct {
   float h_eff;       /* grid spacing of the last step             */
   double zeta;       /* Z of the last step                        */
   double kl;         /* last KL value recorded (kl_every > 0)     */
-  int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow,
-                        8 a bulk copy did not complete in time    */
+  int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
   long nnz;          /* nonzeros of P                             */
   int row_group;     /* lanes per row picked by the autotuner      */
-  int row_kernel;    /* 0: P streamed through L1, 1: P staged in shared
-                        memory by bulk copies (picked by the autotuner) */
+  int row_kernel;    /* attractive SpMV picked by the autotuner: 0 one
+                        block per row tile, 1 persistent blocks walking
+                        one stretch of rows per SM                     */
   float tune_ms[8];  /* row kernel ms measured for 4, 8, 16, 32 lanes,
-                        [0..3] streamed through L1, [4..7] staged      */
+                        [0..3] kernel 0, [4..7] kernel 1               */
 } sgt_job_info;
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
@@ -209,6 +209,49 @@ sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs,
 /* Queue `iters` iterations of every job; asynchronous like sgt_job_run. */
 sgt_status sgt_batch_run(sgt_batch *batch, int iters);
 void sgt_batch_destroy(sgt_batch *batch);
+
+/* ---- one embedding split by rows over ranks (one GPU per rank) ---------
+ * No counterpart in the reference, which runs one embedding on one GPU.
+ * Rank r holds rows row0 .. row0 + nrows - 1 of P (CSR of those rows,
+ * rowptr[0] = 0, column indices over all n_all points), the momentum, gains
+ * and forces of those points, and three caller-owned device buffers that
+ * the caller's collectives (e.g. NCCL) exchange between the phases of an
+ * iteration:
+ *   y_all  n_all points x S floats (S = 1, 2, 4 for d = 1, 2, 3): every
+ *          point's coordinates; the update phase writes the own rows;
+ *   grid   sgt_shard_grid_floats(params) floats: the charge grid;
+ *   zsum   one double: Z.
+ * One iteration, every rank in the same order:
+ *   sgt_shard_scatter   grid decision from all of y_all, S2G of the own
+ *                       points into grid, the own rows' attractive SpMV
+ *   (all-reduce grid, sum)
+ *   sgt_shard_gather    G2G of grid, G2S of the own points, their Z into zsum
+ *   (all-reduce zsum, sum)
+ *   sgt_shard_update    forces, gains, momentum and coordinates of the own
+ *                       rows, written into y_all
+ *   (all-gather the own rows of y_all)
+ * The phases only queue work on the context's stream (no host
+ * synchronisation).  Every rank's sequence of iterations equals the one
+ * embedding's: the grid, Z and schedule are global.  CSR only; no relayout
+ * or in-loop KL.  Replaces, across GPUs, the loop of kl_minimization
+ * (CU/gradient_descend.cu:102-282). */
+typedef struct sgt_shard sgt_shard;
+size_t sgt_shard_grid_floats(const sgt_params *params);
+sgt_status sgt_shard_create(sgt_ctx *ctx, const sgt_params *params, int n_all, int row0,
+                            int nrows, const int *rowptr, const int *col, const float *val,
+                            int mem_is_device, float *y_all, float *grid, size_t grid_floats,
+                            double *zsum, sgt_shard **out);
+void sgt_shard_destroy(sgt_shard *shard);
+/* All n_all points' coordinates (n_all x d, layout), resets the schedule. */
+sgt_status sgt_shard_set_y(sgt_shard *shard, const float *y, int layout, int mem_is_device);
+sgt_status sgt_shard_scatter(sgt_shard *shard);
+sgt_status sgt_shard_gather(sgt_shard *shard);
+sgt_status sgt_shard_update(sgt_shard *shard);
+/* All n_all points' coordinates out of y_all (after the all-gather);
+   synchronises; statuses as sgt_job_get_y. */
+sgt_status sgt_shard_get_y(sgt_shard *shard, float *y, int layout, int mem_is_device,
+                           int centre);
+sgt_status sgt_shard_get_info(sgt_shard *shard, sgt_job_info *info);
 
 /* Device bytes a job of these dimensions holds at its peak (creation
    included); what the server admits against its budget. */
