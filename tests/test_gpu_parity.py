@@ -605,6 +605,41 @@ def test_knn_tensor_filter_matches_simt(torch, ctx, n, dim, k, kind):
         assert redo <= 0.01 * n
 
 
+@pytest.mark.parametrize("kind", ["mixed", "far"])
+def test_knn_tensor_filter_redo_path(torch, ctx, kind):
+    """Queries the filter cannot settle go to the SIMT search.  A query
+    settles when its 64th candidate's approximate distance, minus the error
+    bound 1e-4 (|q|^2 + max |c|^2), exceeds its k-th exact distance.
+    'mixed': half the points in a tight blob (spread 1e-3, distance gaps far
+    below the bound: redone) and half spread wide (spread 10: settled).
+    'far': every point 3000 from the origin, so the bound exceeds every gap
+    and every query is redone.  Either way the result equals the SIMT
+    search bit for bit."""
+    import sgtsne_b200 as S
+    n, dim, k = 5000, 24, 16
+    rng = np.random.default_rng(17)
+    if kind == "mixed":
+        X = rng.standard_normal((n, dim)) * 10.0
+        X[: n // 2] = rng.standard_normal((n // 2, dim)) * 1e-3
+    else:
+        X = rng.standard_normal((n, dim)) + 3000.0
+    X = np.ascontiguousarray(X, np.float32)
+    out = {}
+    for m in (S.KNN_SIMT, S.KNN_TENSOR):
+        idx = torch.full((n * k,), -7, dtype=torch.int32, device="cuda")
+        d2 = torch.full((n * k,), -7.0, dtype=torch.float32, device="cuda")
+        redo = ctx.knn(n, dim, dev(torch, X), k, idx, d2, method=m)
+        out[m] = (idx.cpu().numpy(), d2.cpu().numpy(), redo)
+    (i1, d1, _), (i2, dd2, redo) = out[S.KNN_SIMT], out[S.KNN_TENSOR]
+    print(f"\nknn redo {kind}: {redo} of {n} queries redone by the SIMT search")
+    if kind == "far":
+        assert redo == n
+    else:
+        assert 0 < redo < n
+    assert np.array_equal(i1, i2)
+    assert np.array_equal(d1.view(np.uint32), dd2.view(np.uint32))
+
+
 def test_knn_tensor_rejects_wide_points_and_large_k(torch, ctx):
     import sgtsne_b200 as S
     X = torch.zeros(5000 * 65, dtype=torch.float32, device="cuda")
