@@ -15,6 +15,7 @@
 #include "sgt_prep.cuh"
 #include "sgt_rows.cuh"
 #include "sgt_relayout.cuh"
+#include "sgt_multi.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -185,6 +186,7 @@ void sgt_params_default(sgt_params *p) {
   p->lambda_dist = 1;
   p->seed = 0;
   p->relayout_every = 0;
+  p->locality_order = 1;
 }
 
 int sgt_abi_version(void) { return SGT_ABI_VERSION; }
@@ -945,6 +947,62 @@ static sgt_status relayout_d(sgt_job *J) {
   return SGT_OK;
 }
 
+// diffusion steps of the initial locality order (more steps flatten the
+// structure inside clusters onto the cluster means)
+#define SGT_DIFFUSE_STEPS 10
+#define SGT_ORDER_MIN_N 65536
+
+// The job's first order: P, the per-point state and the caller <-> engine
+// permutation relabelled along the Morton order of diffusion coordinates
+// (see sgt_relayout.cuh).  Runs at creation, before the first sgt_job_set_y,
+// so Ynext and Y are free to hold the coordinates.
+template <int D>
+static sgt_status locality_order_d(sgt_job *J) {
+  sgt_ctx *ctx = J->ctx;
+  cudaStream_t s = ctx->stream;
+  typedef typename Vec<D>::T VT;
+  const int n = J->n;
+  VT *za = (VT *)J->Ynext, *zb = (VT *)J->Y;
+  k_diffuse_init<D><<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(za, n);
+  for (int t = 0; t < SGT_DIFFUSE_STEPS; t++) {
+    k_diffuse<D><<<grid_blocks(ctx->nsm, 8), SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, za, zb, n);
+    std::swap(za, zb);
+  }
+  CK(cudaGetLastError());
+  if (za != (VT *)J->Ynext)
+    CK(cudaMemcpyAsync(J->Ynext, za, sizeof(VT) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemsetAsync(J->st, 0, sizeof(SgtState), s));
+  CKS(init_stats(J, s, 1));  // the lattice of the Morton keys spans these coordinates
+  CKS(relayout_d<D>(J));
+  J->relayouts = 0;  // counts the relabellings during the run
+  if (J->p.relayout_every <= 0) {
+    // no relabelling during the run: give back the scratch of the relabelling
+    void *scratch[] = {J->rowptr_alt, J->pairs_alt, J->perm_alt, J->rl_p, J->rl_iperm,
+                       J->rl_len, J->rl_hist, J->rl_bsum, J->rl_keys, J->gains_alt};
+    for (void *q : scratch) {
+      auto it = std::find(J->allocs.begin(), J->allocs.end(), q);
+      if (it != J->allocs.end()) {
+        CK(cudaFreeAsync(q, s));
+        J->allocs.erase(it);
+      }
+    }
+    J->rowptr_alt = J->perm_alt = J->rl_p = J->rl_iperm = J->rl_len = J->rl_hist = J->rl_bsum =
+        nullptr;
+    J->pairs_alt = nullptr;
+    J->rl_keys = nullptr;
+    J->gains_alt = nullptr;
+  }
+  return SGT_OK;
+}
+
+static sgt_status locality_order(sgt_job *J) {
+  switch (J->d) {
+    case 1: return locality_order_d<1>(J);
+    case 2: return locality_order_d<2>(J);
+    default: return locality_order_d<3>(J);
+  }
+}
+
 static sgt_status relayout(sgt_job *J) {
   if (J->format != SGT_FORMAT_CSR || J->n > (16 << 20)) return SGT_OK;
   switch (J->d) {
@@ -1117,6 +1175,11 @@ static sgt_status job_create_impl(sgt_ctx *ctx, const sgt_params *params, int n,
     if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(ctx, SGT_ERR_CUDA, "hybrid upload"));
   }
   if ((st = jalloc(J, &J->Fattr, (size_t)n * J->S)) != SGT_OK) return bail(st);
+  if (J->format == SGT_FORMAT_CSR && params->locality_order > 0 && n >= SGT_ORDER_MIN_N &&
+      ncols == n) {
+    st = locality_order(J);
+    if (st != SGT_OK) return bail(st);
+  }
   if (J->format == SGT_FORMAT_CSR) {
     st = tune_group(J);
     if (st != SGT_OK) return bail(st);
@@ -1324,11 +1387,39 @@ sgt_status sgt_job_run(sgt_job *J, int iters) {
 // ---------------------------------------------------------------------------
 // batches: one graph, one branch of R chained iterations per job
 // ---------------------------------------------------------------------------
+// Fused form: the jobs of one dimension run every stage as one launch
+// (sgt_multi.cuh).  A group holds the view table of its jobs, one prefix
+// table of block counts per stage, and one view/prefix table per row-group
+// lane count for the SpMV.
+enum {
+  FS_BIN_COUNT, FS_BIN_SCAN, FS_BIN_SCATTER, FS_S2G, FS_S2G8, FS_S2G_CELL, FS_FFT_X,
+  FS_FFT_MID_FWD, FS_FFT_LAST, FS_FFT_MID_INV, FS_FFT_FINAL, FS_G2S, FS_UPDATE, FS_STAGES
+};
+struct BatchGroup {
+  int D = 2, njobs = 0;
+  const SgtJobView *views = nullptr;
+  const int *prefix[FS_STAGES] = {};
+  int blocks[FS_STAGES] = {};
+  size_t smem_s2g = 0, smem_s2g8 = 0, smem_fft = 0;
+  // SpMV: one launch per lane count G present
+  struct Spmv {
+    int G = 16, njobs = 0, blocks = 0;
+    const SgtJobView *views = nullptr;
+    const int *prefix = nullptr;
+  };
+  std::vector<Spmv> spmv;
+  cudaStream_t chain = nullptr, side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_spmv = nullptr, ev_done = nullptr;
+};
+
 struct sgt_batch {
   sgt_ctx *ctx = nullptr;
   std::vector<sgt_job *> jobs;
   int R = 1;
   cudaGraphExec_t exec_r = nullptr, exec_1 = nullptr;
+  bool fused = false;
+  std::vector<BatchGroup> groups;
+  void *dmem = nullptr;  // the groups' view and prefix tables
 };
 
 static sgt_status batch_build(sgt_batch *b, const std::vector<cudaGraph_t> &iter_graphs, int R,
@@ -1356,6 +1447,245 @@ static sgt_status batch_build(sgt_batch *b, const std::vector<cudaGraph_t> &iter
   return SGT_OK;
 }
 
+}  // extern "C"
+
+static SgtJobView job_view(const sgt_job *J) {
+  SgtJobView v;
+  memset(&v, 0, sizeof(v));
+  v.Ynext_c = J->Ynext;
+  v.Ynext = J->Ynext;
+  v.Y = J->Y;
+  v.uY = J->uY;
+  v.gains = J->gains;
+  v.Frep = J->Frep;
+  v.Fattr = J->Fattr;
+  v.sorted = J->sorted;
+  v.V = J->V;
+  v.Phi = J->Phi;
+  v.W = J->W;
+  v.tile_count = J->tile_count;
+  v.cursor = J->cursor;
+  v.chunks = J->chunks;
+  v.part_min = J->part_min;
+  v.part_max = J->part_max;
+  v.part_sum = J->part_sum;
+  v.part_z = J->part_z;
+  v.st = J->st;
+  v.rowptr = J->rowptr;
+  v.pairs = J->pairs;
+  v.jp = J->jp;
+  v.n = J->n;
+  v.nb_s2g = J->nb_s2g;
+  v.row0 = J->row0;
+  return v;
+}
+
+// blocks a job launches in each stage (0: the stage does not exist for it)
+static void stage_blocks(const sgt_job *J, int *b) {
+  for (int k = 0; k < FS_STAGES; k++) b[k] = 0;
+  b[FS_BIN_COUNT] = J->nb_pts;
+  b[FS_BIN_SCAN] = 1;
+  b[FS_BIN_SCATTER] = J->nb_pts;
+  b[FS_S2G] = J->nb_s2g;
+  if (J->d == 3) b[FS_S2G8] = J->nb_s2g8;
+  b[FS_S2G_CELL] = J->nb_s2gc;
+  b[FS_FFT_X] = J->d == 1 ? 1 : J->nb_fft_rows;
+  if (J->d == 3) b[FS_FFT_MID_FWD] = b[FS_FFT_MID_INV] = J->nb_fft;
+  if (J->d >= 2) {
+    b[FS_FFT_LAST] = J->nb_fft;
+    b[FS_FFT_FINAL] = J->nb_fft_rows;
+  }
+  b[FS_G2S] = J->nb_g2s;
+  b[FS_UPDATE] = J->nb_upd;
+}
+
+static sgt_status batch_fused_tables(sgt_batch *b) {
+  sgt_ctx *ctx = b->ctx;
+  // host images of every table, then one upload
+  std::vector<SgtJobView> views;
+  std::vector<int> ints;
+  struct Off {
+    size_t views, prefix[FS_STAGES];
+    std::vector<std::pair<size_t, size_t>> spmv;  // (views, prefix) per G
+  };
+  std::vector<Off> offs;
+  for (int D = 1; D <= 3; D++) {
+    std::vector<sgt_job *> js;
+    for (sgt_job *J : b->jobs)
+      if (J->d == D) js.push_back(J);
+    if (js.empty()) continue;
+    BatchGroup g;
+    g.D = D;
+    g.njobs = (int)js.size();
+    Off o;
+    o.views = views.size();
+    for (sgt_job *J : js) {
+      views.push_back(job_view(J));
+      g.smem_s2g = std::max(g.smem_s2g, J->smem_s2g);
+      g.smem_s2g8 = std::max(g.smem_s2g8, J->smem_s2g8);
+      g.smem_fft = std::max(g.smem_fft, J->smem_fft2);
+    }
+    for (int k = 0; k < FS_STAGES; k++) {
+      o.prefix[k] = ints.size();
+      int acc = 0;
+      ints.push_back(0);
+      for (sgt_job *J : js) {
+        int bl[FS_STAGES];
+        stage_blocks(J, bl);
+        acc += bl[k];
+        ints.push_back(acc);
+      }
+      g.blocks[k] = acc;
+    }
+    for (int G : {4, 8, 16, 32}) {
+      std::vector<sgt_job *> gj;
+      for (sgt_job *J : js)
+        if (J->G == G) gj.push_back(J);
+      if (gj.empty()) continue;
+      BatchGroup::Spmv sp;
+      sp.G = G;
+      sp.njobs = (int)gj.size();
+      const size_t vo = views.size(), po = ints.size();
+      int acc = 0;
+      ints.push_back(0);
+      for (sgt_job *J : gj) {
+        views.push_back(job_view(J));
+        acc += (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
+        ints.push_back(acc);
+      }
+      sp.blocks = acc;
+      g.spmv.push_back(sp);
+      o.spmv.push_back({vo, po});
+    }
+    b->groups.push_back(g);
+    offs.push_back(o);
+  }
+  const size_t vbytes = sizeof(SgtJobView) * views.size();
+  const size_t ibytes = sizeof(int) * ints.size();
+  CK(cudaMallocAsync(&b->dmem, vbytes + ibytes, ctx->stream));
+  CK(cudaMemcpyAsync(b->dmem, views.data(), vbytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync((char *)b->dmem + vbytes, ints.data(), ibytes, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const SgtJobView *dv = (const SgtJobView *)b->dmem;
+  const int *di = (const int *)((char *)b->dmem + vbytes);
+  for (size_t q = 0; q < b->groups.size(); q++) {
+    BatchGroup &g = b->groups[q];
+    g.views = dv + offs[q].views;
+    for (int k = 0; k < FS_STAGES; k++) g.prefix[k] = di + offs[q].prefix[k];
+    for (size_t t = 0; t < g.spmv.size(); t++) {
+      g.spmv[t].views = dv + offs[q].spmv[t].first;
+      g.spmv[t].prefix = di + offs[q].spmv[t].second;
+    }
+    CK(cudaStreamCreateWithFlags(&g.chain, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&g.ev_spmv, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&g.ev_done, cudaEventDisableTiming));
+  }
+  return SGT_OK;
+}
+
+#define FL(k) g.blocks[k], SGT_THREADS
+template <int D>
+static sgt_status enqueue_fused_group(sgt_ctx *ctx, BatchGroup &g) {
+  cudaStream_t c = g.chain, sd = g.side;
+  const SgtJobView *v = g.views;
+  const int nj = g.njobs;
+  // attractive SpMV of every job, beside the repulsion chain
+  for (const BatchGroup::Spmv &sp : g.spmv) {
+    switch (sp.G) {
+      case 4: km_attr_rows<D, 4><<<sp.blocks, SGT_THREADS, 0, sd>>>(sp.views, sp.prefix, sp.njobs); break;
+      case 8: km_attr_rows<D, 8><<<sp.blocks, SGT_THREADS, 0, sd>>>(sp.views, sp.prefix, sp.njobs); break;
+      case 16: km_attr_rows<D, 16><<<sp.blocks, SGT_THREADS, 0, sd>>>(sp.views, sp.prefix, sp.njobs); break;
+      default: km_attr_rows<D, 32><<<sp.blocks, SGT_THREADS, 0, sd>>>(sp.views, sp.prefix, sp.njobs); break;
+    }
+  }
+  CK(cudaEventRecord(g.ev_spmv, sd));
+  km_bin_count<D><<<FL(FS_BIN_COUNT), 0, c>>>(v, g.prefix[FS_BIN_COUNT], nj);
+  km_bin_scan<<<g.blocks[FS_BIN_SCAN], 1024, 0, c>>>(v, g.prefix[FS_BIN_SCAN], nj);
+  km_bin_scatter<D><<<FL(FS_BIN_SCATTER), 0, c>>>(v, g.prefix[FS_BIN_SCATTER], nj);
+  constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  km_s2g<D, TT><<<FL(FS_S2G), g.smem_s2g, c>>>(v, g.prefix[FS_S2G], nj);
+  if constexpr (D == 3) km_s2g<3, 8><<<FL(FS_S2G8), g.smem_s2g8, c>>>(v, g.prefix[FS_S2G8], nj);
+  km_s2g_cell<D><<<FL(FS_S2G_CELL), 0, c>>>(v, g.prefix[FS_S2G_CELL], nj);
+  if constexpr (D == 1) {
+    km_conv1d<<<g.blocks[FS_FFT_X], 32, 0, c>>>(v, g.prefix[FS_FFT_X], nj);
+  } else {
+    km_fft_build_x<D><<<FL(FS_FFT_X), 0, c>>>(v, g.prefix[FS_FFT_X], nj);
+    if constexpr (D == 3)
+      km_fft_cols<D, MODE_MID_FWD><<<FL(FS_FFT_MID_FWD), g.smem_fft, c>>>(v, g.prefix[FS_FFT_MID_FWD], nj);
+    km_fft_cols<D, MODE_LAST><<<FL(FS_FFT_LAST), g.smem_fft, c>>>(v, g.prefix[FS_FFT_LAST], nj);
+    if constexpr (D == 3)
+      km_fft_cols<D, MODE_MID_INV><<<FL(FS_FFT_MID_INV), g.smem_fft, c>>>(v, g.prefix[FS_FFT_MID_INV], nj);
+    km_fft_final_x<D><<<FL(FS_FFT_FINAL), 0, c>>>(v, g.prefix[FS_FFT_FINAL], nj);
+  }
+  km_g2s<D><<<FL(FS_G2S), 0, c>>>(v, g.prefix[FS_G2S], nj);
+  CK(cudaStreamWaitEvent(c, g.ev_spmv, 0));
+  km_row_update<D><<<FL(FS_UPDATE), 0, c>>>(v, g.prefix[FS_UPDATE], nj);
+  CK(cudaGetLastError());
+  return SGT_OK;
+}
+#undef FL
+
+// R iterations of every job, captured: per iteration the groups run side by
+// side, each group's SpMV beside its repulsion chain
+static sgt_status batch_fused_graph(sgt_batch *b, int R, cudaGraphExec_t *exec) {
+  sgt_ctx *ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  sgt_status es = SGT_OK;
+  for (int r = 0; r < R && es == SGT_OK; r++) {
+    for (BatchGroup &g : b->groups) {
+      if (cudaEventRecord(g.ev_fork, s) != cudaSuccess ||
+          cudaStreamWaitEvent(g.chain, g.ev_fork, 0) != cudaSuccess ||
+          cudaStreamWaitEvent(g.side, g.ev_fork, 0) != cudaSuccess) {
+        es = fail(ctx, SGT_ERR_CUDA, "batch capture: fork");
+        break;
+      }
+      switch (g.D) {
+        case 1: es = enqueue_fused_group<1>(ctx, g); break;
+        case 2: es = enqueue_fused_group<2>(ctx, g); break;
+        default: es = enqueue_fused_group<3>(ctx, g); break;
+      }
+      if (es != SGT_OK) break;
+      if (cudaEventRecord(g.ev_done, g.chain) != cudaSuccess) es = fail(ctx, SGT_ERR_CUDA, "batch capture: join");
+    }
+    for (BatchGroup &g : b->groups)
+      if (es == SGT_OK && cudaStreamWaitEvent(s, g.ev_done, 0) != cudaSuccess)
+        es = fail(ctx, SGT_ERR_CUDA, "batch capture: join");
+  }
+  const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+  if (es != SGT_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return es;
+  }
+  CK(ce);
+  const cudaError_t ie = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  CK(ie);
+  return SGT_OK;
+}
+
+template <int D>
+static sgt_status fused_attributes(sgt_ctx *ctx, const BatchGroup &g) {
+  constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  CK(cudaFuncSetAttribute(km_s2g<D, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_s2g));
+  if constexpr (D == 3)
+    CK(cudaFuncSetAttribute(km_s2g<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_s2g8));
+  if constexpr (D >= 2) {
+    CK(cudaFuncSetAttribute(km_fft_cols<D, MODE_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_fft));
+    if constexpr (D == 3) {
+      CK(cudaFuncSetAttribute(km_fft_cols<D, MODE_MID_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_fft));
+      CK(cudaFuncSetAttribute(km_fft_cols<D, MODE_MID_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_fft));
+    }
+  }
+  return SGT_OK;
+}
+
+extern "C" {
+
 sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int iters_per_launch,
                             sgt_batch **out) {
   if (!ctx || !out || njobs < 1 || !jobs || iters_per_launch < 1 || iters_per_launch > 256)
@@ -1372,6 +1702,28 @@ sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int i
   b->ctx = ctx;
   b->jobs.assign(jobs, jobs + njobs);
   b->R = iters_per_launch;
+  // every job in CSR: one launch per stage over all jobs of a dimension
+  bool all_csr = true;
+  for (int k = 0; k < njobs; k++) all_csr = all_csr && jobs[k]->format == SGT_FORMAT_CSR;
+  if (all_csr) {
+    b->fused = true;
+    sgt_status st = batch_fused_tables(b);
+    for (size_t q = 0; q < b->groups.size() && st == SGT_OK; q++) {
+      switch (b->groups[q].D) {
+        case 1: st = fused_attributes<1>(ctx, b->groups[q]); break;
+        case 2: st = fused_attributes<2>(ctx, b->groups[q]); break;
+        default: st = fused_attributes<3>(ctx, b->groups[q]); break;
+      }
+    }
+    if (st == SGT_OK) st = batch_fused_graph(b, b->R, &b->exec_r);
+    if (st == SGT_OK && b->R > 1) st = batch_fused_graph(b, 1, &b->exec_1);
+    if (st != SGT_OK) {
+      sgt_batch_destroy(b);
+      return st;
+    }
+    *out = b;
+    return SGT_OK;
+  }
   std::vector<cudaGraph_t> gs;
   sgt_status st = SGT_OK;
   for (int k = 0; k < njobs && st == SGT_OK; k++) {
@@ -1408,6 +1760,14 @@ void sgt_batch_destroy(sgt_batch *b) {
   cudaSetDevice(b->ctx->device);
   if (b->exec_r) cudaGraphExecDestroy(b->exec_r);
   if (b->exec_1) cudaGraphExecDestroy(b->exec_1);
+  for (BatchGroup &g : b->groups) {
+    if (g.chain) cudaStreamDestroy(g.chain);
+    if (g.side) cudaStreamDestroy(g.side);
+    if (g.ev_fork) cudaEventDestroy(g.ev_fork);
+    if (g.ev_spmv) cudaEventDestroy(g.ev_spmv);
+    if (g.ev_done) cudaEventDestroy(g.ev_done);
+  }
+  if (b->dmem) cudaFreeAsync(b->dmem, b->ctx->stream);
   delete b;
 }
 
@@ -1670,6 +2030,15 @@ size_t sgt_job_footprint(const sgt_params *p, int n, long nnz) {
   if (p->format == SGT_FORMAT_CSR) {
     b += ((size_t)nnz + 8) * 8 + np * 4;  // pairs, Fattr
     transient = std::max(transient, 2 * np * 4);
+    if (p->locality_order > 0 && n >= SGT_ORDER_MIN_N) {
+      b += (size_t)n * 4;  // caller <-> engine permutation
+      // relabelling scratch: the relabelled P, its rowptr, permutations,
+      // keys and the key histogram (held through the run when the job also
+      // relabels during it)
+      const size_t rl = ((size_t)nnz + 8) * 8 + (size_t)n * (24 + 4 * S) + ((size_t)1 << 20) * 4;
+      if (p->relayout_every > 0) b += rl;
+      else transient = std::max(transient, rl);
+    }
   } else if (p->format == SGT_FORMAT_COO) {
     b += 12 * (size_t)nnz + np * 4;  // rows, cols, vals; Fattr
   } else {

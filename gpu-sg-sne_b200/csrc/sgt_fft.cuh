@@ -217,8 +217,7 @@ __device__ void conv1d_body(const SgtState *st, const float2 *__restrict__ V, fl
   }
 }
 
-__global__ void __launch_bounds__(SGT_THREADS)
-k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi) {
+__device__ __forceinline__ void k_conv1d_body(int vb_, int vg_, const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi) {
   __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
@@ -227,6 +226,10 @@ k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ 
   SGT_FFT_DISPATCH(st->M, C1)
 #undef C1
 }
+__global__ void __launch_bounds__(SGT_THREADS)
+k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi) {
+  k_conv1d_body(blockIdx.x, gridDim.x, st, V, Phi);
+}
 
 // ---------------------------------------------------------------------------
 // d >= 2, pass 1: build rows (x lines) of the data planes (rows y, z < N) and
@@ -234,7 +237,7 @@ k_conv1d(const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ 
 // W plane p at W + p * M^d; the kernel plane is p = 2.
 // ---------------------------------------------------------------------------
 template <int D, int M>
-__device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *__restrict__ V,
+__device__ void build_rows_body(int vb_, int vg_, const SgtState *st, const typename Node<D>::T *__restrict__ V,
                                 float2 *__restrict__ W, const float2 *tw) {
   constexpr int E = M / 32;
   const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -243,7 +246,7 @@ __device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *_
   const int nz_d = D == 3 ? N : 1, nz_k = D == 3 ? M : 1;
   const long lines_d = 2L * N * nz_d, lines = lines_d + (long)M * nz_k;
   const int wpb = blockDim.x >> 5;
-  for (long ln = (long)blockIdx.x * wpb + warp; ln < lines; ln += (long)gridDim.x * wpb) {
+  for (long ln = (long)vb_ * wpb + warp; ln < lines; ln += (long)vg_ * wpb) {
     float2 v[E];
     int p, y, z;
     if (ln < lines_d) {
@@ -273,14 +276,18 @@ __device__ void build_rows_body(const SgtState *st, const typename Node<D>::T *_
 }
 
 template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
+__device__ __forceinline__ void k_fft_build_x_body(int vb_, int vg_, const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
   __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
-#define CB(L) build_rows_body<D, L>(st, V, W, tw)
+#define CB(L) build_rows_body<D, L>(vb_, vg_, st, V, W, tw)
   SGT_FFT_DISPATCH(st->M, CB)
 #undef CB
+}
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
+  k_fft_build_x_body<D>(blockIdx.x, gridDim.x, st, V, W);
 }
 
 // ---------------------------------------------------------------------------
@@ -314,7 +321,7 @@ __device__ __forceinline__ void stage_store(const float2 *stg, float2 *__restric
 }
 
 template <int D, int MODE, int M>
-__device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const float2 *tw,
+__device__ void cols_body(int vb_, int vg_, const SgtState *st, float2 *__restrict__ W, const float2 *tw,
                           float2 *stg, float *kre) {
   constexpr int E = M / 32, LS = M + SGT_FFT_PAD;
   const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -327,7 +334,7 @@ __device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const floa
   else if (MODE == MODE_MID_FWD) items = (long)ncb * (2L * N + M);  // data z < N, kernel all z
   else items = (long)ncb * 2L * N;
   float2 v[E];
-  for (long it = blockIdx.x; it < items; it += gridDim.x) {
+  for (long it = vb_; it < items; it += vg_) {
     const int cb = (int)(it % ncb);
     const long rest = it / ncb;
     __syncthreads();
@@ -396,17 +403,21 @@ __device__ void cols_body(const SgtState *st, float2 *__restrict__ W, const floa
 }
 
 template <int D, int MODE>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
+__device__ __forceinline__ void k_fft_cols_body(int vb_, int vg_, const SgtState *st, float2 *__restrict__ W) {
   extern __shared__ float2 sm[];
   float2 *tw = sm;
   float2 *stg = sm + SGT_FFT_MAXM;
   float *kre = reinterpret_cast<float *>(stg + SGT_FFT_COLS * (st->M + SGT_FFT_PAD));
   fft_twiddles(tw, st->M);
   __syncthreads();
-#define CC(L) cols_body<D, MODE, L>(st, W, tw, stg, kre)
+#define CC(L) cols_body<D, MODE, L>(vb_, vg_, st, W, tw, stg, kre)
   SGT_FFT_DISPATCH(st->M, CC)
 #undef CC
+}
+template <int D, int MODE>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
+  k_fft_cols_body<D, MODE>(blockIdx.x, gridDim.x, st, W);
 }
 
 // ---------------------------------------------------------------------------
@@ -414,7 +425,7 @@ k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
 // the potential grid (channels packed per node: plane 0 -> .xy, 1 -> .zw).
 // ---------------------------------------------------------------------------
 template <int D, int M>
-__device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W,
+__device__ void final_rows_body(int vb_, int vg_, const SgtState *st, const float2 *__restrict__ W,
                                 float2 *__restrict__ Phi2, const float2 *tw) {
   constexpr int E = M / 32;
   const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -424,7 +435,7 @@ __device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W
   float inv = 1.0f / (float)M;
   inv = inv / (float)M;
   if (D == 3) inv = inv / (float)M;
-  for (long ln = (long)blockIdx.x * wpb + warp; ln < lines; ln += (long)gridDim.x * wpb) {
+  for (long ln = (long)vb_ * wpb + warp; ln < lines; ln += (long)vg_ * wpb) {
     const int p = (int)(ln % 2);
     const long r = ln / 2;
     const int y = (int)(r % N), z = D == 3 ? (int)(r / N) : 0;
@@ -443,14 +454,18 @@ __device__ void final_rows_body(const SgtState *st, const float2 *__restrict__ W
 }
 
 template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_fft_final_x(const SgtState *st, const float2 *__restrict__ W, typename Node<D>::T *__restrict__ Phi) {
+__device__ __forceinline__ void k_fft_final_x_body(int vb_, int vg_, const SgtState *st, const float2 *__restrict__ W, typename Node<D>::T *__restrict__ Phi) {
   __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
-#define CF(L) final_rows_body<D, L>(st, W, reinterpret_cast<float2 *>(Phi), tw)
+#define CF(L) final_rows_body<D, L>(vb_, vg_, st, W, reinterpret_cast<float2 *>(Phi), tw)
   SGT_FFT_DISPATCH(st->M, CF)
 #undef CF
+}
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_fft_final_x(const SgtState *st, const float2 *__restrict__ W, typename Node<D>::T *__restrict__ Phi) {
+  k_fft_final_x_body<D>(blockIdx.x, gridDim.x, st, W, Phi);
 }
 
 // shared memory of a column pass for FFT length Mmax

@@ -195,8 +195,7 @@ k_init_stats(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
 // bin_count: centre (Y = Ynext - mean), zero the grid V, count points per tile
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
+__device__ __forceinline__ void k_bin_count_body(int vb_, int vg_, const typename Vec<D>::T *__restrict__ Ynext,
             typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
             int *__restrict__ tile_count, typename Node<D>::T *__restrict__ V,
             int write_centred) {
@@ -213,16 +212,16 @@ k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
   if (D >= 3) nodes *= N;
   typename Node<D>::T z;
   if constexpr (D == 1) z = make_float2(0.f, 0.f); else z = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < nodes;
-       g += (long)gridDim.x * blockDim.x)
+  for (long g = vb_ * (long)blockDim.x + threadIdx.x; g < nodes;
+       g += (long)vg_ * blockDim.x)
     V[g] = z;
   __syncthreads();
   // warp-uniform trip count: lanes with the same tile are merged with
   // match_any and add their count in one shared-memory atomic (points of an
   // embedding cluster on few tiles)
   const int lane = threadIdx.x & 31;
-  const long stride = (long)gridDim.x * blockDim.x;
-  for (long i0 = (long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
+  const long stride = (long)vg_ * blockDim.x;
+  for (long i0 = (long)vb_ * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
     const int i = (int)i0 + lane;
     int key = -1;
     if (i < n) {
@@ -245,6 +244,14 @@ k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
     if (hist[t]) atomicAdd(&tile_count[t], hist[t]);
+}
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
+            typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+            int *__restrict__ tile_count, typename Node<D>::T *__restrict__ V,
+            int write_centred) {
+  k_bin_count_body<D>(blockIdx.x, gridDim.x, Ynext, Y, n, st, tile_count, V, write_centred);
 }
 
 // ---------------------------------------------------------------------------
@@ -277,8 +284,7 @@ __device__ __forceinline__ int block_exclusive_scan_1024(int v, int *total) {
   return excl;
 }
 
-__global__ void __launch_bounds__(1024)
-k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
+__device__ __forceinline__ void k_bin_scan_body(int vb_, int vg_, SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
            int *__restrict__ cursor, int4 *__restrict__ chunks, int nblk) {
   const int ntiles = st->ntiles;
   // chunk length: about two chunks per persistent CTA, at least 1024 points
@@ -325,6 +331,11 @@ k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
     st->nchunks = tot_ch;
   }
 }
+__global__ void __launch_bounds__(1024)
+k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
+           int *__restrict__ cursor, int4 *__restrict__ chunks, int nblk) {
+  k_bin_scan_body(blockIdx.x, gridDim.x, st, jp, tile_count, cursor, chunks, nblk);
+}
 
 // ---------------------------------------------------------------------------
 // bin_scatter: counting-sort points into tile order.  Each CTA owns a
@@ -334,8 +345,7 @@ k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
 // keeps the same slot: idx is always stored in .w).
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_bin_scatter(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+__device__ __forceinline__ void k_bin_scatter_body(int vb_, int vg_, const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
               int *__restrict__ cursor, float4 *__restrict__ sorted) {
   __shared__ int lc[SGT_HIST_MAX];
   const int ntiles = st->ntiles, T = st->T, td = st->tiles_dim;
@@ -343,8 +353,8 @@ k_bin_scatter(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
   float miny[3];
 #pragma unroll
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
-  const int per = (n + gridDim.x - 1) / gridDim.x;
-  const int lo = blockIdx.x * per, hi = min(n, lo + per);
+  const int per = (n + vg_ - 1) / vg_;
+  const int lo = vb_ * per, hi = min(n, lo + per);
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x) lc[t] = 0;
   __syncthreads();
   // warp-uniform trip counts; lanes of one tile are merged with match_any,
@@ -396,6 +406,12 @@ k_bin_scatter(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
     if (key >= 0) sorted[base + __popc(grp & below)] = rec;
   }
 }
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_bin_scatter(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+              int *__restrict__ cursor, float4 *__restrict__ sorted) {
+  k_bin_scatter_body<D>(blockIdx.x, gridDim.x, Y, n, st, cursor, sorted);
+}
 
 // ---------------------------------------------------------------------------
 // S2G over chunks of sorted points; one shared-memory tile per chunk.
@@ -416,8 +432,7 @@ __device__ __forceinline__ void sgt_point_stencil(const float4 &rec,
 // TT: the tile edge this instance handles; the instances of the other tile
 // edges (and k_s2g_cell in cell mode) return at once.
 template <int D, int TT>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_s2g(const float4 *__restrict__ sorted, SgtState *st,
+__device__ __forceinline__ void k_s2g_body(int vb_, int vg_, const float4 *__restrict__ sorted, SgtState *st,
       const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
   extern __shared__ float acc[];  // [D+1][R^D]
   const int T = st->T, td = st->tiles_dim, N = st->N, nch = st->nchunks;
@@ -435,7 +450,7 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
   if (D >= 2) RD *= R;
   if (D >= 3) RD *= R;
   constexpr int m = D + 1;
-  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+  for (int c = vb_; c < nch; c += vg_) {
     const int4 ch = chunks[c];
     int o[3] = {0, 0, 0};
     o[0] = (ch.x % td) * T;
@@ -567,6 +582,12 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
     __syncthreads();
   }
 }
+template <int D, int TT>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_s2g(const float4 *__restrict__ sorted, SgtState *st,
+      const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
+  k_s2g_body<D, TT>(blockIdx.x, gridDim.x, sorted, st, chunks, V);
+}
 
 // ---------------------------------------------------------------------------
 // S2G in cell mode (T = 1): every point of a chunk lies in the chunk's cell,
@@ -576,8 +597,7 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
 // d = 3 runs in four passes over the z offset of the stencil (64 sums each).
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
+__device__ __forceinline__ void k_s2g_cell_body(int vb_, int vg_, const float4 *__restrict__ sorted, SgtState *st,
            const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
   if (st->T != 1) return;  // tile mode: k_s2g does the work
   constexpr int NN = D == 1 ? 4 : 16;  // stencil nodes per pass
@@ -594,7 +614,7 @@ k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
   float *Vf = reinterpret_cast<float *>(V);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+  for (int c = vb_; c < nch; c += vg_) {
     const int4 ch = chunks[c];
     int cf[3] = {0, 0, 0};
     cf[0] = ch.x % td;
@@ -654,14 +674,19 @@ k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
     }
   }
 }
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
+           const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
+  k_s2g_cell_body<D>(blockIdx.x, gridDim.x, sorted, st, chunks, V);
+}
 
 // ---------------------------------------------------------------------------
 // G2S over chunks + repulsive force numerator + Z (FP64, fixed-order finish).
 // Frep_un[i] = y_i*Phi0 - Phi_{1..d}; Z = sum_i z_i - n.
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_g2s(const float4 *__restrict__ sorted, SgtState *st,
+__device__ __forceinline__ void k_g2s_body(int vb_, int vg_, const float4 *__restrict__ sorted, SgtState *st,
       const int4 *__restrict__ chunks,
       const typename Node<D>::T *__restrict__ Phi,
       typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n) {
@@ -674,7 +699,7 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
 #pragma unroll
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
   double zacc = 0.0;
-  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+  for (int c = vb_; c < nch; c += vg_) {
     const int4 ch = chunks[c];
     for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
       const float4 rec = sorted[j];
@@ -723,15 +748,15 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
   if (threadIdx.x == 0) {
     double s = 0;
     for (int k = 0; k < SGT_THREADS / 32; k++) s += wz[k];
-    part_z[blockIdx.x] = s;
+    part_z[vb_] = s;
     __threadfence();
-    last = (atomicAdd(&st->done_g2s, 1u) == gridDim.x - 1);
+    last = (atomicAdd(&st->done_g2s, 1u) == vg_ - 1);
   }
   __syncthreads();
   if (last) {
     __threadfence();
     double s = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(&part_z[b]);
+    for (int b = threadIdx.x; b < (int)vg_; b += blockDim.x) s += __ldcg(&part_z[b]);
     s = warp_sum_d(s);
     __syncthreads();
     if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = s;
@@ -743,6 +768,14 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
       st->done_g2s = 0;
     }
   }
+}
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_g2s(const float4 *__restrict__ sorted, SgtState *st,
+      const int4 *__restrict__ chunks,
+      const typename Node<D>::T *__restrict__ Phi,
+      typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n) {
+  k_g2s_body<D>(blockIdx.x, gridDim.x, sorted, st, chunks, Phi, Frep_un, part_z, n);
 }
 
 // ---------------------------------------------------------------------------

@@ -185,3 +185,67 @@ __global__ void k_gather_vec(const typename Vec<D>::T *__restrict__ src, const i
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
     dst[r] = src[p[r]];
 }
+
+// ---- the locality order a job starts from ---------------------------------
+// Points are ordered once, at job creation, by the Morton code of coordinates
+// from a few diffusion steps over P's graph: start from random coordinates
+// and replace every point's coordinates by the P-weighted mean of its
+// neighbours' a few times.  Neighbours in P end up with nearby coordinates
+// (as in a diffusion map; the few steps keep the structure inside clusters,
+// which more steps would flatten onto the cluster means), so the Morton
+// order of these coordinates puts the neighbours of a row near it in memory
+// before the embedding itself has any structure.
+
+// uniform [-1, 1) from the point index (splitmix64)
+__device__ __forceinline__ float sgt_hash_unit(unsigned long long x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return (float)(x >> 40) * (1.0f / 8388608.0f) - 1.0f;
+}
+
+template <int D>
+__global__ void k_diffuse_init(typename Vec<D>::T *__restrict__ z, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    typename Vec<D>::T v;
+    if constexpr (D == 3) v.w = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; k++) setcomp<D>(v, k, sgt_hash_unit((unsigned long long)i * 3 + k));
+    z[i] = v;
+  }
+}
+
+// one diffusion step, a warp per row: zout_i = sum_j p_ij zin_j / sum_j p_ij
+template <int D>
+__global__ void k_diffuse(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+                          const typename Vec<D>::T *__restrict__ zin,
+                          typename Vec<D>::T *__restrict__ zout, int n) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * blockDim.x / 32;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < n; i += warps) {
+    float acc[3] = {0.f, 0.f, 0.f}, w = 0.f;
+    for (int t = rowptr[i] + lane; t < rowptr[i + 1]; t += 32) {
+      const int2 pr = pairs[t];
+      const float p = __int_as_float(pr.y);
+      const typename Vec<D>::T zj = zin[pr.x];
+#pragma unroll
+      for (int k = 0; k < D; k++) acc[k] += p * comp<D>(zj, k);
+      w += p;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      w += __shfl_xor_sync(0xffffffffu, w, o);
+#pragma unroll
+      for (int k = 0; k < D; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    }
+    if (lane == 0) {
+      typename Vec<D>::T v = zin[i];
+      if (w > 0.f) {
+#pragma unroll
+        for (int k = 0; k < D; k++) setcomp<D>(v, k, acc[k] / w);
+      }
+      zout[i] = v;
+    }
+  }
+}

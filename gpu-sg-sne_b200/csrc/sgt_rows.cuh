@@ -83,7 +83,7 @@ __device__ __forceinline__ float sgn_f(float x) {
 // Per-block min/max/sum of Ynext -> partials; the last block reduces all
 // partials with every thread and turns them into the next grid decision.
 template <int D>
-__device__ __forceinline__ void block_finish_stats(SgtState *st, const SgtJobParams &jp,
+__device__ __forceinline__ void block_finish_stats(int vb_, int vg_, SgtState *st, const SgtJobParams &jp,
                                                    float *mn, float *mx, double *sm,
                                                    float4 *part_min, float4 *part_max,
                                                    double *part_sum, int iter, float alpha,
@@ -108,18 +108,18 @@ __device__ __forceinline__ void block_finish_stats(SgtState *st, const SgtJobPar
       if (D > 1) { a.y = fminf(a.y, smin[j][1]); b.y = fmaxf(b.y, smax[j][1]); s[1] += ssum[j][1]; }
       if (D > 2) { a.z = fminf(a.z, smin[j][2]); b.z = fmaxf(b.z, smax[j][2]); s[2] += ssum[j][2]; }
     }
-    part_min[blockIdx.x] = a;
-    part_max[blockIdx.x] = b;
-    for (int k = 0; k < 3; k++) part_sum[blockIdx.x * 4 + k] = s[k];
+    part_min[vb_] = a;
+    part_max[vb_] = b;
+    for (int k = 0; k < 3; k++) part_sum[vb_ * 4 + k] = s[k];
     __threadfence();
-    last = (atomicAdd(&st->done_row, 1u) == gridDim.x - 1);
+    last = (atomicAdd(&st->done_row, 1u) == vg_ - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   double s[3] = {0, 0, 0};
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+  for (int b = threadIdx.x; b < (int)vg_; b += blockDim.x) {
     const float4 a = __ldcg(&part_min[b]), c = __ldcg(&part_max[b]);
     lo[0] = fminf(lo[0], a.x); hi[0] = fmaxf(hi[0], c.x);
     lo[1] = fminf(lo[1], a.y); hi[1] = fmaxf(hi[1], c.y);
@@ -165,8 +165,7 @@ __device__ __forceinline__ void block_finish_stats(SgtState *st, const SgtJobPar
 // turns the per-block min/max/sum of Ynext into the next grid decision.
 // ---------------------------------------------------------------------------
 template <int D, int G, bool FUSED>
-__global__ void __launch_bounds__(SGT_THREADS)
-k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+__device__ __forceinline__ void k_row_update_body(int vb_, int vg_, const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
              const typename Vec<D>::T *__restrict__ Fattr,
              const typename Vec<D>::T *__restrict__ Y,
              const typename Vec<D>::T *__restrict__ Frep_un,
@@ -184,8 +183,8 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
   float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
   double sm[3] = {0, 0, 0};
   const int lane = threadIdx.x % G;
-  const int grp = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const int ngrp = gridDim.x * blockDim.x / G;
+  const int grp = (vb_ * blockDim.x + threadIdx.x) / G;
+  const int ngrp = vg_ * blockDim.x / G;
   // uniform trip count per warp so the group shuffles stay converged
   const int rounds = (n + ngrp - 1) / ngrp;
   // the next row's extents are loaded one round ahead
@@ -259,7 +258,20 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
       Ynext[i] = yn;
     }
   }
-  block_finish_stats<D>(st, jp, mn, mx, sm, part_min, part_max, part_sum, iter, alpha, mom);
+  block_finish_stats<D>(vb_, vg_, st, jp, mn, mx, sm, part_min, part_max, part_sum, iter, alpha, mom);
+}
+template <int D, int G, bool FUSED>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+             const typename Vec<D>::T *__restrict__ Fattr,
+             const typename Vec<D>::T *__restrict__ Y,
+             const typename Vec<D>::T *__restrict__ Frep_un,
+             typename Vec<D>::T *__restrict__ uY,
+             typename Vec<D>::T *__restrict__ gains,
+             typename Vec<D>::T *__restrict__ Ynext, SgtState *st,
+             SgtJobParams jp, float4 *part_min, float4 *part_max,
+             double *part_sum) {
+  k_row_update_body<D, G, FUSED>(blockIdx.x, gridDim.x, rowptr, pairs, Fattr, Y, Frep_un, uY, gains, Ynext, st, jp, part_min, part_max, part_sum);
 }
 
 
@@ -274,12 +286,11 @@ k_row_update(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 // with global column indices and gathers from the whole Y).
 // ---------------------------------------------------------------------------
 template <int D, int G>
-__global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
-k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+__device__ __forceinline__ void k_attr_rows_body(int vb_, int vg_, const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
             const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
             int n, int row0) {
   const int lane = threadIdx.x % G;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int i = (vb_ * blockDim.x + threadIdx.x) / G;
   const bool valid = i < n;
   float acc[3] = {0.f, 0.f, 0.f};
   if (valid) {
@@ -294,6 +305,13 @@ k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
     for (int k = 0; k < D; k++) setcomp<D>(f, k, acc[k]);
     Fattr[i] = f;
   }
+}
+template <int D, int G>
+__global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
+k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
+            const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
+            int n, int row0) {
+  k_attr_rows_body<D, G>(blockIdx.x, gridDim.x, rowptr, pairs, Y, Fattr, n, row0);
 }
 
 // ---------------------------------------------------------------------------

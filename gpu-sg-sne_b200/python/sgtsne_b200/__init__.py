@@ -48,7 +48,8 @@ class Params(C.Structure):
                 ("format", C.c_int), ("bs", C.c_int), ("compute_error", C.c_int),
                 ("ng", C.c_int), ("sim", C.c_int), ("grid_mode", C.c_int),
                 ("lambda_dist", C.c_int), ("max_grid", C.c_int), ("kl_every", C.c_int),
-                ("seed", C.c_uint64), ("relayout_every", C.c_int)]
+                ("seed", C.c_uint64), ("relayout_every", C.c_int),
+                ("locality_order", C.c_int)]
 
 
 class JobInfo(C.Structure):

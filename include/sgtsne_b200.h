@@ -91,11 +91,17 @@ typedef struct {
                          their grid cells every this many iterations
                          (memory locality of the attractive term; results
                          are returned in the caller's order).  0 = off    */
+  int locality_order; /* 1 (default): a CSR job of at least 65,536 points
+                         starts from a locality order of its points: the
+                         Morton order of a few diffusion steps over P's
+                         graph, so the attractive term's gathers stay near
+                         each row from the first iteration (results are
+                         returned in the caller's order).  0 = off        */
 } sgt_params;
 
 /* Fill *p with the reference defaults (d=2, lambda=1, alpha=12,
    max_iter=1000, early_iter=250, h=-1, format=SGT_FORMAT_COO, ng=50);
-   relayout_every = 0. */
+   relayout_every = 0, locality_order = 1. */
 void sgt_params_default(sgt_params *p);
 
 typedef struct sgt_ctx sgt_ctx;
