@@ -91,6 +91,7 @@ struct SgtJobParams {
   int mmax;           // largest FFT length per axis allocated
   int tile_cap;       // max tiles held by the tile arrays
   int chunk_cap;      // max chunks held by the chunk array
+  int chunk_min;      // fewest points per S2G chunk (0: 1024, 256 in 3-D)
 };
 
 template <int D> struct Vec;

@@ -39,6 +39,11 @@ struct sgt_ctx {
   sgt_job *scratch = nullptr;  // buffers of the operator entry points
   int scratch_n = 0, scratch_d = 0;
   int last_N = 0, last_d = 0;
+  // sgt_batch_step: device tables of the fused launches (grown as needed)
+  // and the fork/join events of up to three dimension groups
+  void *step_tables = nullptr;
+  size_t step_bytes = 0;
+  cudaEvent_t step_ev[9] = {};
 };
 
 struct sgt_job {
@@ -253,6 +258,12 @@ void sgt_destroy(sgt_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->scratch) sgt_job_destroy(ctx->scratch);
+  if (ctx->step_tables) {
+    cudaFreeAsync(ctx->step_tables, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  for (cudaEvent_t e : ctx->step_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   delete ctx;
@@ -1449,6 +1460,8 @@ static sgt_status batch_build(sgt_batch *b, const std::vector<cudaGraph_t> &iter
 
 }  // extern "C"
 
+static void stage_blocks(const sgt_job *J, int *b, int *nb_s2g2 = nullptr);
+
 static SgtJobView job_view(const sgt_job *J) {
   SgtJobView v;
   memset(&v, 0, sizeof(v));
@@ -1475,65 +1488,87 @@ static SgtJobView job_view(const sgt_job *J) {
   v.pairs = J->pairs;
   v.jp = J->jp;
   v.n = J->n;
-  v.nb_s2g = J->nb_s2g;
+  int bl[FS_STAGES];
+  stage_blocks(J, bl, &v.nb_s2g);  // the binning sizes chunks for the fused S2G grid
+  // short chunks: a chunk is one block's serial work in S2G, and in a fused
+  // launch the slowest block of the smallest jobs sets the stage's length
+  v.jp.chunk_min = 256;
   v.row0 = J->row0;
   return v;
 }
 
-// blocks a job launches in each stage (0: the stage does not exist for it)
-static void stage_blocks(const sgt_job *J, int *b) {
+// Blocks a job gets in each stage of a fused launch (0: the stage does not
+// exist for it).  A job launched alone sizes its grids to fill the GPU; in
+// a fused launch its blocks share the GPU with every other job's, so each
+// job gets blocks in proportion to its work instead (the kernels loop over
+// whatever they are given): a block per 2048 points in the point passes and
+// per 2048 points of chunks in S2G and G2S, up to the job's own grid, and the
+// FFT passes a block per 8 lines of a 64-point grid (they loop over larger
+// ones).  nb_s2g2 is the S2G block count the binning sizes its chunks for.
+static void stage_blocks(const sgt_job *J, int *b, int *nb_s2g2) {
   for (int k = 0; k < FS_STAGES; k++) b[k] = 0;
-  b[FS_BIN_COUNT] = J->nb_pts;
+  const int work = std::max(1, (J->n + 2047) / 2048);
+  const int s2g = std::min(J->nb_s2g, work);
+  b[FS_BIN_COUNT] = std::min(J->nb_pts, work);
   b[FS_BIN_SCAN] = 1;
-  b[FS_BIN_SCATTER] = J->nb_pts;
-  b[FS_S2G] = J->nb_s2g;
-  if (J->d == 3) b[FS_S2G8] = J->nb_s2g8;
-  b[FS_S2G_CELL] = J->nb_s2gc;
-  b[FS_FFT_X] = J->d == 1 ? 1 : J->nb_fft_rows;
-  if (J->d == 3) b[FS_FFT_MID_FWD] = b[FS_FFT_MID_INV] = J->nb_fft;
+  b[FS_BIN_SCATTER] = std::min(J->nb_pts, work);
+  b[FS_S2G] = s2g;
+  if (J->d == 3) b[FS_S2G8] = std::min(J->nb_s2g8, 2 * work);
+  b[FS_S2G_CELL] = std::min(J->nb_s2gc, 2 * work);
+  const int rows64 = J->d == 3 ? (2 * 64 * 64 + 128 * 128) / 8 : (2 * 64 + 128) / 8;
+  b[FS_FFT_X] = J->d == 1 ? 1 : std::min(J->nb_fft_rows, rows64);
+  if (J->d == 3) b[FS_FFT_MID_FWD] = b[FS_FFT_MID_INV] = std::min(J->nb_fft, 128);
   if (J->d >= 2) {
-    b[FS_FFT_LAST] = J->nb_fft;
-    b[FS_FFT_FINAL] = J->nb_fft_rows;
+    b[FS_FFT_LAST] = std::min(J->nb_fft, J->d == 3 ? 128 : 16);
+    b[FS_FFT_FINAL] = std::min(J->nb_fft_rows, rows64);
   }
-  b[FS_G2S] = J->nb_g2s;
-  b[FS_UPDATE] = J->nb_upd;
+  b[FS_G2S] = std::min(J->nb_g2s, 2 * work);
+  b[FS_UPDATE] = std::min(J->nb_upd, work);
+  if (nb_s2g2) *nb_s2g2 = s2g;
 }
 
-static sgt_status batch_fused_tables(sgt_batch *b) {
-  sgt_ctx *ctx = b->ctx;
-  // host images of every table, then one upload
+// Host images of the tables of fused launches over `jobs` (all CSR): the
+// groups by dimension with their block counts, the views and the prefix
+// tables; offsets into the two arrays stand in for device pointers until
+// bind_fused_tables.
+struct FusedImage {
   std::vector<SgtJobView> views;
   std::vector<int> ints;
+  std::vector<BatchGroup> groups;
   struct Off {
-    size_t views, prefix[FS_STAGES];
+    size_t views = 0, prefix[FS_STAGES] = {};
     std::vector<std::pair<size_t, size_t>> spmv;  // (views, prefix) per G
   };
   std::vector<Off> offs;
+  size_t bytes() const { return sizeof(SgtJobView) * views.size() + sizeof(int) * ints.size(); }
+};
+
+static void build_fused_image(const std::vector<sgt_job *> &jobs, FusedImage &im) {
   for (int D = 1; D <= 3; D++) {
     std::vector<sgt_job *> js;
-    for (sgt_job *J : b->jobs)
+    for (sgt_job *J : jobs)
       if (J->d == D) js.push_back(J);
     if (js.empty()) continue;
     BatchGroup g;
     g.D = D;
     g.njobs = (int)js.size();
-    Off o;
-    o.views = views.size();
+    FusedImage::Off o;
+    o.views = im.views.size();
     for (sgt_job *J : js) {
-      views.push_back(job_view(J));
+      im.views.push_back(job_view(J));
       g.smem_s2g = std::max(g.smem_s2g, J->smem_s2g);
       g.smem_s2g8 = std::max(g.smem_s2g8, J->smem_s2g8);
       g.smem_fft = std::max(g.smem_fft, J->smem_fft2);
     }
     for (int k = 0; k < FS_STAGES; k++) {
-      o.prefix[k] = ints.size();
+      o.prefix[k] = im.ints.size();
       int acc = 0;
-      ints.push_back(0);
+      im.ints.push_back(0);
       for (sgt_job *J : js) {
         int bl[FS_STAGES];
         stage_blocks(J, bl);
         acc += bl[k];
-        ints.push_back(acc);
+        im.ints.push_back(acc);
       }
       g.blocks[k] = acc;
     }
@@ -1545,38 +1580,53 @@ static sgt_status batch_fused_tables(sgt_batch *b) {
       BatchGroup::Spmv sp;
       sp.G = G;
       sp.njobs = (int)gj.size();
-      const size_t vo = views.size(), po = ints.size();
+      const size_t vo = im.views.size(), po = im.ints.size();
       int acc = 0;
-      ints.push_back(0);
+      im.ints.push_back(0);
       for (sgt_job *J : gj) {
-        views.push_back(job_view(J));
+        im.views.push_back(job_view(J));
         acc += (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-        ints.push_back(acc);
+        im.ints.push_back(acc);
       }
       sp.blocks = acc;
       g.spmv.push_back(sp);
       o.spmv.push_back({vo, po});
     }
-    b->groups.push_back(g);
-    offs.push_back(o);
+    im.groups.push_back(g);
+    im.offs.push_back(o);
   }
-  const size_t vbytes = sizeof(SgtJobView) * views.size();
-  const size_t ibytes = sizeof(int) * ints.size();
-  CK(cudaMallocAsync(&b->dmem, vbytes + ibytes, ctx->stream));
-  CK(cudaMemcpyAsync(b->dmem, views.data(), vbytes, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync((char *)b->dmem + vbytes, ints.data(), ibytes, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  const SgtJobView *dv = (const SgtJobView *)b->dmem;
-  const int *di = (const int *)((char *)b->dmem + vbytes);
-  for (size_t q = 0; q < b->groups.size(); q++) {
-    BatchGroup &g = b->groups[q];
-    g.views = dv + offs[q].views;
-    for (int k = 0; k < FS_STAGES; k++) g.prefix[k] = di + offs[q].prefix[k];
+}
+
+// upload the image to `dmem` (image.bytes() bytes) on `s` and point the
+// groups at it
+static sgt_status bind_fused_image(sgt_ctx *ctx, FusedImage &im, void *dmem, cudaStream_t s) {
+  const size_t vbytes = sizeof(SgtJobView) * im.views.size();
+  CK(cudaMemcpyAsync(dmem, im.views.data(), vbytes, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync((char *)dmem + vbytes, im.ints.data(), sizeof(int) * im.ints.size(),
+                     cudaMemcpyHostToDevice, s));
+  const SgtJobView *dv = (const SgtJobView *)dmem;
+  const int *di = (const int *)((char *)dmem + vbytes);
+  for (size_t q = 0; q < im.groups.size(); q++) {
+    BatchGroup &g = im.groups[q];
+    g.views = dv + im.offs[q].views;
+    for (int k = 0; k < FS_STAGES; k++) g.prefix[k] = di + im.offs[q].prefix[k];
     for (size_t t = 0; t < g.spmv.size(); t++) {
-      g.spmv[t].views = dv + offs[q].spmv[t].first;
-      g.spmv[t].prefix = di + offs[q].spmv[t].second;
+      g.spmv[t].views = dv + im.offs[q].spmv[t].first;
+      g.spmv[t].prefix = di + im.offs[q].spmv[t].second;
     }
+  }
+  return SGT_OK;
+}
+
+static sgt_status batch_fused_tables(sgt_batch *b) {
+  sgt_ctx *ctx = b->ctx;
+  FusedImage im;
+  build_fused_image(b->jobs, im);
+  CK(cudaMallocAsync(&b->dmem, im.bytes(), ctx->stream));
+  CKS(bind_fused_image(ctx, im, b->dmem, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));  // the host image goes out of scope
+  b->groups = im.groups;
+  for (BatchGroup &g : b->groups) {
     CK(cudaStreamCreateWithFlags(&g.chain, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
@@ -1685,6 +1735,68 @@ static sgt_status fused_attributes(sgt_ctx *ctx, const BatchGroup &g) {
 }
 
 extern "C" {
+
+sgt_status sgt_batch_step(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int iters) {
+  if (!ctx || njobs < 1 || !jobs || iters < 0) return SGT_ERR_INVALID_ARG;
+  std::vector<sgt_job *> js(jobs, jobs + njobs);
+  for (sgt_job *J : js) {
+    if (!J || J->ctx->device != ctx->device)
+      return fail(ctx, SGT_ERR_INVALID_ARG, "sgt_batch_step: jobs must live on the context's device");
+    if (J->format != SGT_FORMAT_CSR || J->p.relayout_every > 0 || J->p.kl_every > 0 || J->Ygather)
+      return fail(ctx, SGT_ERR_UNSUPPORTED,
+                  "sgt_batch_step: CSR jobs without relayout, in-loop KL or sharding only");
+  }
+  if (iters == 0) return SGT_OK;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  FusedImage im;
+  build_fused_image(js, im);
+  if (im.groups.size() > 3) return fail(ctx, SGT_ERR_UNSUPPORTED, "sgt_batch_step: groups");
+  if (im.bytes() > ctx->step_bytes) {
+    // stream-ordered: the old tables are freed after the launches that read them
+    if (ctx->step_tables) CK(cudaFreeAsync(ctx->step_tables, s));
+    ctx->step_tables = nullptr;
+    ctx->step_bytes = 0;
+    const size_t want = std::max(im.bytes() * 2, (size_t)1 << 16);
+    CK(cudaMallocAsync(&ctx->step_tables, want, s));
+    ctx->step_bytes = want;
+  }
+  CKS(bind_fused_image(ctx, im, ctx->step_tables, s));
+  for (size_t q = 0; q < im.groups.size(); q++) {
+    BatchGroup &g = im.groups[q];
+    for (int e = 0; e < 3; e++)
+      if (!ctx->step_ev[3 * q + e])
+        CK(cudaEventCreateWithFlags(&ctx->step_ev[3 * q + e], cudaEventDisableTiming));
+    g.chain = s;
+    g.side = ctx->side;
+    g.ev_fork = ctx->step_ev[3 * q];
+    g.ev_spmv = ctx->step_ev[3 * q + 1];
+    g.ev_done = ctx->step_ev[3 * q + 2];
+    switch (g.D) {
+      case 1: CKS(fused_attributes<1>(ctx, g)); break;
+      case 2: CKS(fused_attributes<2>(ctx, g)); break;
+      default: CKS(fused_attributes<3>(ctx, g)); break;
+    }
+  }
+  sgt_status st = SGT_OK;
+  for (int it = 0; it < iters && st == SGT_OK; it++) {
+    for (BatchGroup &g : im.groups) {
+      CK(cudaEventRecord(g.ev_fork, s));
+      CK(cudaStreamWaitEvent(g.side, g.ev_fork, 0));
+      switch (g.D) {
+        case 1: st = enqueue_fused_group<1>(ctx, g); break;
+        case 2: st = enqueue_fused_group<2>(ctx, g); break;
+        default: st = enqueue_fused_group<3>(ctx, g); break;
+      }
+      if (st != SGT_OK) break;
+    }
+  }
+  // the groups' views live in ctx->step_tables; their host image goes out
+  // of scope here (the uploads were staged at the call)
+  if (st == SGT_OK)
+    for (sgt_job *J : js) J->host_iter += iters;
+  return st;
+}
 
 sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int iters_per_launch,
                             sgt_batch **out) {

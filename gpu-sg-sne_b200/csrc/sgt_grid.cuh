@@ -292,7 +292,7 @@ __device__ __forceinline__ void k_bin_scan_body(int vb_, int vg_, SgtState *st, 
   // chunks than they have 1024-point runs)
   int chunk = (jp.n + 2 * nblk - 1) / (2 * nblk);
   chunk = ((chunk + 255) / 256) * 256;
-  const int cmin = jp.d == 3 ? 256 : 1024;
+  const int cmin = jp.chunk_min > 0 ? jp.chunk_min : (jp.d == 3 ? 256 : 1024);
   if (chunk < cmin) chunk = cmin;
   const int per = (ntiles + 1023) / 1024;  // <= 4
   int cnt[4], cpt[4];

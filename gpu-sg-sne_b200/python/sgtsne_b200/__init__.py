@@ -97,6 +97,7 @@ SIGNATURES = {
     "sgt_batch_create": (_i, [_vp, _i, C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "sgt_batch_run": (_i, [_vp, _i]),
     "sgt_batch_destroy": (None, [_vp]),
+    "sgt_batch_step": (_i, [_vp, _i, C.POINTER(_vp), _i]),
     "sgt_job_footprint": (C.c_size_t, [C.POINTER(Params), _i, _l]),
     "sgt_server_config_default": (None, [C.POINTER(ServerConfig)]),
     "sgt_server_create": (_i, [_i, C.POINTER(ServerConfig), C.POINTER(_vp)]),

@@ -212,9 +212,21 @@ sgt_status sgt_job_repulsive_error(sgt_job *job, double *rel_err);
 typedef struct sgt_batch sgt_batch;
 sgt_status sgt_batch_create(sgt_ctx *ctx, int njobs, sgt_job *const *jobs,
                             int iters_per_launch, sgt_batch **out);
-/* Queue `iters` iterations of every job; asynchronous like sgt_job_run. */
+/* Queue `iters` iterations of every job; asynchronous like sgt_job_run.
+   When every job holds P in CSR, each stage of an iteration is one launch
+   over all jobs of a dimension (blocks mapped to jobs through a table of
+   their block counts), so a batch takes about a dozen launches per
+   iteration whatever its job count; otherwise the graph has one branch of
+   chained iterations per job. */
 sgt_status sgt_batch_run(sgt_batch *batch, int iters);
 void sgt_batch_destroy(sgt_batch *batch);
+/* The same fused launches without a batch object or graph: queue `iters`
+   iterations of the given jobs (CSR, no relayout or in-loop KL) on ctx's
+   stream, for a set of jobs that changes from call to call (the server's
+   rounds).  Jobs may belong to other contexts of the same device; their
+   streams must have finished the jobs' earlier work (the caller orders
+   them, e.g. with events). */
+sgt_status sgt_batch_step(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int iters);
 
 /* ---- one embedding split by rows over ranks (one GPU per rank) ---------
  * No counterpart in the reference, which runs one embedding on one GPU.
@@ -269,10 +281,11 @@ size_t sgt_job_footprint(const sgt_params *params, int n, long nnz);
  * priority rises as n falls, so short requests are not stuck behind long
  * ones).  An admission thread turns waiting requests into jobs, in FIFO
  * order, as soon as their footprint fits the budget and a slot is free; a
- * scheduler thread keeps every running job `rounds_ahead` rounds of
- * `iters_per_round` iterations ahead of the GPU (one graph launch per
- * round), copies a finished job's coordinates to the caller's buffer and
- * returns its memory to the budget.  Requests that arrive while others run
+ * scheduler thread runs rounds in which every running job advances by up to
+ * `iters_per_round` iterations through fused launches over all of them
+ * (sgt_batch_step), keeps `rounds_ahead` rounds queued, adds jobs as they
+ * become ready, copies a finished job's coordinates to the caller's buffer
+ * and returns its memory to the budget.  Requests that arrive while others run
  * are admitted while those are still on the GPU; their kernels overlap. */
 typedef struct sgt_server sgt_server;
 typedef struct {
@@ -305,7 +318,9 @@ void sgt_server_destroy(sgt_server *srv);
    (as sgt_job_create); y0 and y_out: host, point-major n*d.  All caller-owned
    and kept alive until the request is done or failed.  params->max_iter is
    the number of iterations; the result is centred as after the reference's
-   last iteration.  *id receives the request id (0, 1, 2, ...). */
+   last iteration.  params->format must be SGT_FORMAT_CSR (the rounds run
+   every job through the fused launches of sgt_batch_step), without
+   relayout or in-loop KL.  *id receives the request id (0, 1, 2, ...). */
 sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n,
                              const int *rowptr, const int *col,
                              const float *val, const float *y0, float *y_out,

@@ -105,6 +105,36 @@ def test_batch_matches_alone(problems, oracle, iters):
     ctx.close()
 
 
+def test_batch_of_mixed_formats(problems):
+    """A batch holding a COO job runs one graph branch per job instead of the
+    fused launches of an all-CSR batch; results match alone runs."""
+    import sgtsne_b200 as S
+    ctx = S.Context(0)
+    fmts = [S.FORMAT_CSR, S.FORMAT_COO, S.FORMAT_CSR]
+    alone, jobs = [], []
+    for prob, fmt in zip(problems[:3], fmts):
+        rp, col, val, d, y0 = prob
+        p = params(S, d, SHORT)
+        p.format = fmt
+        for dest in (alone, jobs):
+            j = S.Job(ctx, p, rp, col, val, device_mem=False)
+            j.set_y(y0, S.LAYOUT_POINT_MAJOR, False)
+            dest.append(j)
+    for j in alone:
+        j.run(SHORT)
+    batch = S.Batch(ctx, jobs, iters_per_launch=1)
+    batch.run(SHORT)
+    for a, j, prob in zip(alone, jobs, problems):
+        ya, yb = np.empty_like(prob[4]), np.empty_like(prob[4])
+        a.get_y(ya, S.LAYOUT_POINT_MAJOR, False, 1)
+        j.get_y(yb, S.LAYOUT_POINT_MAJOR, False, 1)
+        assert rel(yb, ya) <= TOL_Y
+    batch.close()
+    for j in alone + jobs:
+        j.close()
+    ctx.close()
+
+
 def test_batch_rejects_foreign_and_relayout(problems):
     import sgtsne_b200 as S
     c1, c2 = S.Context(0), S.Context(0)
@@ -232,7 +262,13 @@ def test_one_dimensional_batch_and_server(problems):
         j.close()
     ctx.close()
     srv = S.Server(0, max_active=2, iters_per_round=4)
-    outs = [srv.submit(par(fmt, SHORT), rp, col, val, y0)[1] for rp, col, val, y0, fmt in probs]
+    # the server runs requests in CSR (fused rounds); other formats are refused
+    rp, col, val, y0, _ = probs[1]
+    with pytest.raises(S.SgtError) as e:
+        srv.submit(par(S.FORMAT_COO, SHORT), rp, col, val, y0)
+    assert e.value.status == 4
+    outs = [srv.submit(par(S.FORMAT_CSR, SHORT), rp, col, val, y0)[1]
+            for rp, col, val, y0, _ in probs]
     done = []
     for _ in range(300):
         done += srv.poll(wait_ms=50)

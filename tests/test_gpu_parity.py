@@ -351,6 +351,33 @@ def test_relayout_is_transparent(torch, ctx):
     assert rel(out[10], out[0]) <= 1e-4
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_locality_order_is_transparent(torch, ctx, oracle, d):
+    """A job of at least 65,536 points starts from the diffusion locality
+    order of its P (locality_order = 1, the default); the caller sees the
+    embedding of locality_order = 0 in its own point order (rel-L2 <= 1e-5
+    after 2 iterations: only the order of FP32 atomics differs)."""
+    import sgtsne_b200 as S
+    n, k = 70000, 10
+    rng = np.random.default_rng(21)
+    col = rng.integers(0, n - 1, (n, k))
+    col += col >= np.arange(n)[:, None]  # no self loops
+    rp = (np.arange(n + 1) * k).astype(np.int32)
+    v = rng.random(n * k) + 0.1
+    srp, sc, sv = oracle.symmetrize(rp, col.reshape(-1).astype(np.int32), v, 1.0 / (2 * n))
+    Y0 = (rng.standard_normal((n, d)) * 1e-2).astype(np.float32)
+    out = {}
+    for order in (0, 1):
+        p = S.default_params(d=d, format=S.FORMAT_CSR)
+        p.locality_order = order
+        job = S.Job(ctx, p, srp, sc, sv.astype(np.float32), device_mem=False)
+        job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+        job.run(2)
+        out[order] = job.get_y(np.empty((n, d), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        job.close()
+    assert rel(out[1], out[0]) <= 1e-5
+
+
 @pytest.mark.parametrize("d", [1, 2, 3])
 def test_repulsive_error_probe(torch, ctx, oracle, d):
     """sgt_job_repulsive_error (the -f probe of CU/compute_error.cu:80-99):
