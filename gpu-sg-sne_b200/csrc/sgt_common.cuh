@@ -18,10 +18,6 @@
 #define SGT_MAX_GRID 512        // largest grid (points per axis) of the size table
 #define SGT_FFT_LINES 8         // lines per CTA in the FFT axis passes
 #define SGT_THREADS 256
-// index of a row-group lane count G in {4, 8, 16, 32}
-__host__ __device__ constexpr int sgt_group_index(int G) {
-  return G == 4 ? 0 : (G == 8 ? 1 : (G == 16 ? 2 : 3));
-}
 
 // Lagrange cubic weights on 4 nodes (CU/gridding.cuh:13-22,
 // HYB/gridding.cpp:29-39).  Node f+a gets w[a]; the point lies between

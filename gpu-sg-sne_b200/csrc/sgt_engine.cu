@@ -96,13 +96,7 @@ struct sgt_job {
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
   double last_kl = 0.0;
-  // row kernel ms for G = 4, 8, 16, 32 with one block per row tile
-  // ([0..3], k_attr_rows) and with persistent blocks walking per-SM
-  // stretches of rows ([4..7], k_attr_rows_sm)
-  float tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int sm_rows = 0;             // 1: the attractive SpMV is k_attr_rows_sm
-  unsigned *sm_ctr = nullptr;  // its per-stretch tile counters (SGT_SM_SLOTS + 1)
-  int nb_rows_sm[4] = {0, 0, 0, 0};  // its persistent grid for G = 4, 8, 16, 32
+  float tune_ms[4] = {0, 0, 0, 0};  // row kernel ms for G = 4, 8, 16, 32
 };
 
 // ---------------------------------------------------------------------------
@@ -626,12 +620,8 @@ static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   const VT *Yc = (const VT *)(J->Ygather ? J->Ygather : J->Ynext);
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (J->sm_rows)
-      k_attr_rows_sm<D, G><<<J->nb_rows_sm[sgt_group_index(G)], SGT_THREADS, 0, s>>>(
-          J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n, J->row0, J->sm_ctr);
-    else
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
-                                                   J->row0);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
+                                                 J->row0);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals, Yc,
@@ -808,20 +798,15 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
 // fastest of G = 4, 8, 16, 32 is kept.
 // ---------------------------------------------------------------------------
 template <int D, int G>
-static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1,
-                       bool sm) {
+static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1) {
   typedef typename Vec<D>::T VT;
   cudaStream_t s = J->ctx->stream;
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {  // the first launch warms caches
     cudaEventRecord(e0, s);
     const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (sm)
-      k_attr_rows_sm<D, G><<<J->nb_rows_sm[sgt_group_index(G)], SGT_THREADS, 0, s>>>(
-          J->rowptr, J->pairs, (const VT *)tY, (VT *)tF, J->n, J->row0, J->sm_ctr);
-    else
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
-                                                   (VT *)tF, J->n, J->row0);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY, (VT *)tF,
+                                                 J->n, J->row0);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -843,29 +828,14 @@ static sgt_status tune_group_d(sgt_job *J) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  CKS(jalloc(J, &J->sm_ctr, (size_t)SGT_SM_SLOTS + 1));
-  CK(cudaMemsetAsync(J->sm_ctr, 0, sizeof(unsigned) * (SGT_SM_SLOTS + 1), s));
-  {  // persistent grids of k_attr_rows_sm: every block resident at once
-    int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 4>, SGT_THREADS, 0));
-    J->nb_rows_sm[0] = grid_blocks(ctx->nsm, occ);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 8>, SGT_THREADS, 0));
-    J->nb_rows_sm[1] = grid_blocks(ctx->nsm, occ);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 16>, SGT_THREADS, 0));
-    J->nb_rows_sm[2] = grid_blocks(ctx->nsm, occ);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_attr_rows_sm<D, 32>, SGT_THREADS, 0));
-    J->nb_rows_sm[3] = grid_blocks(ctx->nsm, occ);
-  }
   const float *tY = buf;  // zero coordinates: the gather pattern of P, finite values
   float *tF = buf + np;
   const int cand[4] = {4, 8, 16, 32};
-  float t[8];
-  for (int b = 0; b < 2; b++) {
-    t[4 * b + 0] = time_spmv<D, 4>(J, tY, tF, e0, e1, b == 1);
-    t[4 * b + 1] = time_spmv<D, 8>(J, tY, tF, e0, e1, b == 1);
-    t[4 * b + 2] = time_spmv<D, 16>(J, tY, tF, e0, e1, b == 1);
-    t[4 * b + 3] = time_spmv<D, 32>(J, tY, tF, e0, e1, b == 1);
-  }
+  float t[4];
+  t[0] = time_spmv<D, 4>(J, tY, tF, e0, e1);
+  t[1] = time_spmv<D, 8>(J, tY, tF, e0, e1);
+  t[2] = time_spmv<D, 16>(J, tY, tF, e0, e1);
+  t[3] = time_spmv<D, 32>(J, tY, tF, e0, e1);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -873,11 +843,10 @@ static sgt_status tune_group_d(sgt_job *J) {
   CK(e);
   CK(cudaGetLastError());
   int best = 0;
-  for (int k = 1; k < 8; k++)
+  for (int k = 1; k < 4; k++)
     if (t[k] < t[best]) best = k;
-  J->G = cand[best % 4];
-  J->sm_rows = best >= 4;
-  for (int k = 0; k < 8; k++) J->tune_ms[k] = t[k];
+  J->G = cand[best];
+  for (int k = 0; k < 4; k++) J->tune_ms[k] = t[k];
   return SGT_OK;
 }
 
@@ -1291,12 +1260,6 @@ static bool is_attractive_kernel(const void *f) {
       (const void *)k_attr_rows<2, 16>, (const void *)k_attr_rows<2, 32>,
       (const void *)k_attr_rows<3, 4>, (const void *)k_attr_rows<3, 8>,
       (const void *)k_attr_rows<3, 16>, (const void *)k_attr_rows<3, 32>,
-      (const void *)k_attr_rows_sm<1, 4>, (const void *)k_attr_rows_sm<1, 8>,
-      (const void *)k_attr_rows_sm<1, 16>, (const void *)k_attr_rows_sm<1, 32>,
-      (const void *)k_attr_rows_sm<2, 4>, (const void *)k_attr_rows_sm<2, 8>,
-      (const void *)k_attr_rows_sm<2, 16>, (const void *)k_attr_rows_sm<2, 32>,
-      (const void *)k_attr_rows_sm<3, 4>, (const void *)k_attr_rows_sm<3, 8>,
-      (const void *)k_attr_rows_sm<3, 16>, (const void *)k_attr_rows_sm<3, 32>,
       (const void *)k_attr_ell<1>, (const void *)k_attr_ell<2>, (const void *)k_attr_ell<3>,
       (const void *)k_attr_coo<1>, (const void *)k_attr_coo<2>, (const void *)k_attr_coo<3>};
   for (const void *g : fs)
@@ -2202,8 +2165,7 @@ sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
   info->error_flags = J->st_host->error;
   info->nnz = J->nnz;
   info->row_group = J->G;
-  info->row_kernel = J->sm_rows;
-  for (int k = 0; k < 8; k++) info->tune_ms[k] = J->tune_ms[k];
+  for (int k = 0; k < 4; k++) info->tune_ms[k] = J->tune_ms[k];
   return SGT_OK;
 }
 

@@ -315,79 +315,6 @@ k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 }
 
 // ---------------------------------------------------------------------------
-// The same SpMV as a persistent kernel whose SMs each walk one contiguous
-// stretch of rows.  A block reads the id of the SM it runs on and takes row
-// tiles (SGT_THREADS / G rows) from that SM's stretch through one counter
-// per stretch, then from the stretches that follow once its own is done.
-// The blocks resident on one SM therefore work on neighbouring rows at any
-// time, and when the points are ordered for locality (relabelled) the
-// coordinates their rows gather stay in that SM's L1; k_attr_rows instead
-// spreads consecutive blocks over all SMs.  The last block to finish clears
-// the counters for the next launch.  ctr holds SGT_SM_SLOTS + 1 zeros.
-// ---------------------------------------------------------------------------
-#define SGT_SM_SLOTS 512
-
-template <int D, int G>
-__global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
-k_attr_rows_sm(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
-               const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
-               int n, int row0, unsigned *__restrict__ ctr) {
-  constexpr int RPB = SGT_THREADS / G;
-  __shared__ int s_tile;
-  unsigned smid, nsmid;
-  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-  asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsmid));
-  const int ns = (int)min(max(nsmid, 1u), (unsigned)SGT_SM_SLOTS);
-  const int ntiles = (n + RPB - 1) / RPB;
-  int stretch = (int)(smid % (unsigned)ns), visited = 0;  // used by thread 0 only
-  const int lane = threadIdx.x % G;
-  while (true) {
-    if (threadIdx.x == 0) {
-      int tile = -1;
-      while (visited < ns) {
-        const int lo = (int)((long)stretch * ntiles / ns);
-        const int hi = (int)((long)(stretch + 1) * ntiles / ns);
-        const int k = lo < hi ? (int)atomicAdd(&ctr[stretch], 1u) : hi - lo;
-        if (k < hi - lo) {
-          tile = lo + k;
-          break;
-        }
-        stretch = stretch + 1 == ns ? 0 : stretch + 1;
-        visited++;
-      }
-      s_tile = tile;
-    }
-    __syncthreads();
-    const int tile = s_tile;
-    __syncthreads();  // s_tile is written again in the next round
-    if (tile < 0) break;
-    const int i = tile * RPB + threadIdx.x / G;
-    const bool valid = i < n;
-    float acc[3] = {0.f, 0.f, 0.f};
-    if (valid) {
-      const typename Vec<D>::T yi = Y[row0 + i];
-      csr_row_sum<D, G>(rowptr, pairs, Y, i, lane, yi, acc);
-    }
-    group_reduce<D, G>(acc);
-    if (valid && lane == 0) {
-      typename Vec<D>::T f;
-      if constexpr (D == 3) f.w = 0.f;
-#pragma unroll
-      for (int k = 0; k < D; k++) setcomp<D>(f, k, acc[k]);
-      Fattr[i] = f;
-    }
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(&ctr[SGT_SM_SLOTS], 1u) == gridDim.x - 1) {
-      for (int k = 0; k < ns; k++) ctr[k] = 0u;
-      ctr[SGT_SM_SLOTS] = 0u;
-      __threadfence();
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Attractive term only (operator entry points and the COO/ELL formats).
 // ---------------------------------------------------------------------------
 template <int D, int G>

@@ -5,18 +5,23 @@
 //              footprint fits the HBM budget and a slot is free, builds its
 //              job (P upload, autotune, Y0) on a stream of its own and hands
 //              it to the scheduler with an event that marks it ready;
-//   scheduler  runs rounds: every running job advances by the same number of
+//   scheduler  runs the small jobs (fewer than SGT_SERVE_SMALL points) in
+//              rounds: every one of them advances by the same number of
 //              iterations (at most `iters_per_round`, at most what any of
 //              them has left) through sgt_batch_step, which issues each
-//              stage of an iteration as one launch over all of them.  It
-//              keeps `rounds_ahead` rounds queued, admits newly ready jobs
-//              into the next round, and when the round holding a job's last
-//              iteration has run, copies its coordinates to the caller's
-//              buffer, frees its memory (stream-ordered, no device
-//              synchronisation) and returns its footprint to the budget.
-// Jobs therefore share the GPU from the round after they are ready, whatever
-// their size or arrival time, and a round costs about a dozen launches per
-// iteration however many jobs it holds.
+//              stage of an iteration as one launch over all of them; their
+//              iterations are short and launch-bound alone.  Large jobs are
+//              throughput-bound alone: each runs its own captured iteration
+//              graphs on its own stream (stream priority rising as n falls),
+//              beside the rounds.  The scheduler keeps `rounds_ahead` rounds
+//              (and graph rounds per large job) queued, adds newly ready
+//              jobs, and when a job's last iteration has run, copies its
+//              coordinates to the caller's buffer, frees its memory
+//              (stream-ordered, no device synchronisation) and returns its
+//              footprint to the budget.
+// Jobs therefore share the GPU as soon as they are ready, whatever their
+// size or arrival time; a round costs about a dozen launches per iteration
+// however many small jobs it holds.
 //
 // Only the public C ABI of the engine is used (sgt_job_*, sgt_batch_step),
 // plus the CUDA runtime for streams and events.
@@ -54,8 +59,12 @@ struct Request {
   struct Slot *slot = nullptr;
   sgt_job *job = nullptr;
   int iters_total = 0, iters_queued = 0;
-  cudaEvent_t ready = nullptr;  // recorded on the slot's stream after set_y
+  cudaEvent_t ready = nullptr;       // recorded on the slot's stream after set_y
+  std::deque<cudaEvent_t> inflight;  // a large job's queued graph rounds
 };
+
+// jobs of at least this many points run their own graphs beside the rounds
+constexpr int SGT_SERVE_SMALL = 65536;
 
 // a queued round: its completion event and the requests whose last
 // iteration it holds
@@ -232,6 +241,27 @@ void admission_loop(sgt_server *srv) {
   for (cudaEvent_t e : pool) cudaEventDestroy(e);
 }
 
+// a large job's next graph round on its own stream, with an event
+sgt_status queue_own_round(Request *r, int iters_per_round, std::vector<cudaEvent_t> &pool) {
+  const int k = std::min(iters_per_round, r->iters_total - r->iters_queued);
+  sgt_status st = sgt_job_run(r->job, k);
+  if (st != SGT_OK) return st;
+  cudaEvent_t ev = nullptr;
+  if (!pool.empty()) {
+    ev = pool.back();
+    pool.pop_back();
+  } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    return SGT_ERR_CUDA;
+  }
+  if (cudaEventRecord(ev, r->slot->stream) != cudaSuccess) {
+    pool.push_back(ev);
+    return SGT_ERR_CUDA;
+  }
+  r->inflight.push_back(ev);
+  r->iters_queued += k;
+  return SGT_OK;
+}
+
 // the request leaves: coordinates to the caller once `after` has run on the
 // rounds' stream, job freed on its own stream
 void retire(sgt_server *srv, Request *r, cudaEvent_t after, sgt_status st) {
@@ -246,7 +276,8 @@ void retire(sgt_server *srv, Request *r, cudaEvent_t after, sgt_status st) {
 
 void scheduler_loop(sgt_server *srv) {
   cudaSetDevice(srv->device);
-  std::vector<Request *> running;  // jobs with iterations left to queue
+  std::vector<Request *> running;  // small jobs with iterations left to queue
+  std::vector<Request *> large;    // large jobs, on their own streams
   std::deque<Round> rounds;        // queued rounds, oldest first
   std::vector<cudaEvent_t> pool;
   std::vector<sgt_job *> batch;
@@ -255,16 +286,22 @@ void scheduler_loop(sgt_server *srv) {
     std::vector<Request *> fresh;
     {
       std::unique_lock<std::mutex> lk(srv->mu);
-      if (running.empty() && rounds.empty())
+      if (running.empty() && rounds.empty() && large.empty())
         srv->cv_sched.wait(lk, [&] {
           return !srv->ready.empty() || (srv->stop && srv->active == 0);
         });
       fresh.swap(srv->ready);
       idle_stop = srv->stop && srv->active == 0;
     }
-    if (fresh.empty() && running.empty() && rounds.empty() && idle_stop) break;
+    if (fresh.empty() && running.empty() && rounds.empty() && large.empty() && idle_stop) break;
     bool progress = !fresh.empty();
     for (Request *r : fresh) {
+      if (r->n >= SGT_SERVE_SMALL) {  // runs on its own stream, which holds its upload
+        pool.push_back(r->ready);
+        r->ready = nullptr;
+        large.push_back(r);
+        continue;
+      }
       // the rounds' stream starts on the job once its upload and Y0 are done
       if (cudaStreamWaitEvent(srv->rounds_stream, r->ready, 0) != cudaSuccess) {
         retire(srv, r, nullptr, SGT_ERR_CUDA);
@@ -277,6 +314,29 @@ void scheduler_loop(sgt_server *srv) {
         continue;
       }
       running.push_back(r);
+    }
+    // large jobs: keep `rounds_ahead` graph rounds queued on each job's stream
+    for (size_t q = 0; q < large.size();) {
+      Request *r = large[q];
+      while (!r->inflight.empty() && cudaEventQuery(r->inflight.front()) == cudaSuccess) {
+        pool.push_back(r->inflight.front());
+        r->inflight.pop_front();
+        progress = true;
+      }
+      sgt_status st = SGT_OK;
+      if (r->iters_queued < r->iters_total && (int)r->inflight.size() < srv->cfg.rounds_ahead) {
+        st = queue_own_round(r, srv->cfg.iters_per_round, pool);
+        progress = true;
+      }
+      if (st != SGT_OK || (r->iters_queued == r->iters_total && r->inflight.empty())) {
+        for (cudaEvent_t e : r->inflight) pool.push_back(e);
+        r->inflight.clear();
+        retire(srv, r, nullptr, st);
+        large.erase(large.begin() + q);
+        progress = true;
+        continue;
+      }
+      q++;
     }
     // retire what the finished rounds completed
     while (!rounds.empty() && cudaEventQuery(rounds.front().ev) == cudaSuccess) {
@@ -374,8 +434,10 @@ sgt_status sgt_server_create(int device, const sgt_server_config *cfg, sgt_serve
     srv->prio_least = srv->prio_greatest = 0;
   }
   sgt_status cs = sgt_create(device, &srv->rounds);
-  if (cs == SGT_OK && cudaStreamCreateWithFlags(&srv->rounds_stream, cudaStreamNonBlocking) !=
-                          cudaSuccess)
+  // the rounds of small jobs get the greatest priority: short iterations
+  // should not queue behind the blocks of the large jobs' graphs
+  if (cs == SGT_OK && cudaStreamCreateWithPriority(&srv->rounds_stream, cudaStreamNonBlocking,
+                                                   srv->prio_greatest) != cudaSuccess)
     cs = SGT_ERR_CUDA;
   if (cs == SGT_OK) cs = sgt_set_stream(srv->rounds, srv->rounds_stream);
   if (cs != SGT_OK) {
