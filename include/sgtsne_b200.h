@@ -177,7 +177,10 @@ typedef struct {
   int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
   long nnz;          /* nonzeros of P                             */
   int row_group;     /* lanes per row picked by the autotuner      */
-  float tune_ms[4];  /* row kernel ms measured for 4, 8, 16, 32 lanes */
+  int row_order;     /* 1: the autotuner gave the blocks that share an
+                        SM neighbouring row tiles, 0: index order      */
+  float tune_ms[8];  /* row kernel ms measured for 4, 8, 16, 32 lanes,
+                        [0..3] index order, [4..7] neighbouring tiles */
 } sgt_job_info;
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
