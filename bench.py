@@ -514,9 +514,6 @@ def run_ours(args, rank, world, local, dist):
                        "p_source": p_source, "p_engine_vs_stored": p_match,
                        "grid_points_start": grid_start, "grid_points_end": info.grid_points,
                        "h_eff_end": round(info.h_eff, 5), "row_group": info.row_group,
-                       "row_order": ["blocks in index order",
-                                     "co-resident blocks on neighbouring row tiles"][
-                                         info.row_order],
                        "relayout_every": args.relayout,
                        "row_group_tune_ms": [round(x, 4) for x in info.tune_ms],
                        "l2": "inputs larger than L2 (P >= 400 MB), no flush",

@@ -96,10 +96,7 @@ struct sgt_job {
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
   double last_kl = 0.0;
-  // row kernel ms for G = 4, 8, 16, 32, blocks in index order ([0..3]) and
-  // with the tiles of co-resident blocks side by side ([4..7])
-  float tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int swz = 0;  // 1: the SpMV is k_attr_rows_swz
+  float tune_ms[4] = {0, 0, 0, 0};  // row kernel ms for G = 4, 8, 16, 32
 };
 
 // ---------------------------------------------------------------------------
@@ -623,14 +620,8 @@ static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   const VT *Yc = (const VT *)(J->Ygather ? J->Ygather : J->Ynext);
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (J->swz) {
-      const int st = ctx->nsm, q = (nb + st - 1) / st;
-      k_attr_rows_swz<D, G><<<st * q, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc,
-                                                          (VT *)J->Fattr, n, J->row0, st);
-    } else {
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
-                                                   J->row0);
-    }
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
+                                                 J->row0);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals, Yc,
@@ -807,22 +798,15 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
 // fastest of G = 4, 8, 16, 32 is kept.
 // ---------------------------------------------------------------------------
 template <int D, int G>
-static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1,
-                       bool swz) {
+static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1) {
   typedef typename Vec<D>::T VT;
   cudaStream_t s = J->ctx->stream;
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {  // the first launch warms caches
     cudaEventRecord(e0, s);
     const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (swz) {
-      const int st = J->ctx->nsm, q = (nb + st - 1) / st;
-      k_attr_rows_swz<D, G><<<st * q, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
-                                                          (VT *)tF, J->n, J->row0, st);
-    } else {
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
-                                                   (VT *)tF, J->n, J->row0);
-    }
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY, (VT *)tF,
+                                                 J->n, J->row0);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -847,13 +831,11 @@ static sgt_status tune_group_d(sgt_job *J) {
   const float *tY = buf;  // zero coordinates: the gather pattern of P, finite values
   float *tF = buf + np;
   const int cand[4] = {4, 8, 16, 32};
-  float t[8];
-  for (int w = 0; w < 2; w++) {
-    t[4 * w + 0] = time_spmv<D, 4>(J, tY, tF, e0, e1, w == 1);
-    t[4 * w + 1] = time_spmv<D, 8>(J, tY, tF, e0, e1, w == 1);
-    t[4 * w + 2] = time_spmv<D, 16>(J, tY, tF, e0, e1, w == 1);
-    t[4 * w + 3] = time_spmv<D, 32>(J, tY, tF, e0, e1, w == 1);
-  }
+  float t[4];
+  t[0] = time_spmv<D, 4>(J, tY, tF, e0, e1);
+  t[1] = time_spmv<D, 8>(J, tY, tF, e0, e1);
+  t[2] = time_spmv<D, 16>(J, tY, tF, e0, e1);
+  t[3] = time_spmv<D, 32>(J, tY, tF, e0, e1);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -861,11 +843,10 @@ static sgt_status tune_group_d(sgt_job *J) {
   CK(e);
   CK(cudaGetLastError());
   int best = 0;
-  for (int k = 1; k < 8; k++)
+  for (int k = 1; k < 4; k++)
     if (t[k] < t[best]) best = k;
-  J->G = cand[best % 4];
-  J->swz = best >= 4;
-  for (int k = 0; k < 8; k++) J->tune_ms[k] = t[k];
+  J->G = cand[best];
+  for (int k = 0; k < 4; k++) J->tune_ms[k] = t[k];
   return SGT_OK;
 }
 
@@ -1279,12 +1260,6 @@ static bool is_attractive_kernel(const void *f) {
       (const void *)k_attr_rows<2, 16>, (const void *)k_attr_rows<2, 32>,
       (const void *)k_attr_rows<3, 4>, (const void *)k_attr_rows<3, 8>,
       (const void *)k_attr_rows<3, 16>, (const void *)k_attr_rows<3, 32>,
-      (const void *)k_attr_rows_swz<1, 4>, (const void *)k_attr_rows_swz<1, 8>,
-      (const void *)k_attr_rows_swz<1, 16>, (const void *)k_attr_rows_swz<1, 32>,
-      (const void *)k_attr_rows_swz<2, 4>, (const void *)k_attr_rows_swz<2, 8>,
-      (const void *)k_attr_rows_swz<2, 16>, (const void *)k_attr_rows_swz<2, 32>,
-      (const void *)k_attr_rows_swz<3, 4>, (const void *)k_attr_rows_swz<3, 8>,
-      (const void *)k_attr_rows_swz<3, 16>, (const void *)k_attr_rows_swz<3, 32>,
       (const void *)k_attr_ell<1>, (const void *)k_attr_ell<2>, (const void *)k_attr_ell<3>,
       (const void *)k_attr_coo<1>, (const void *)k_attr_coo<2>, (const void *)k_attr_coo<3>};
   for (const void *g : fs)
@@ -2190,8 +2165,7 @@ sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
   info->error_flags = J->st_host->error;
   info->nnz = J->nnz;
   info->row_group = J->G;
-  info->row_order = J->swz;
-  for (int k = 0; k < 8; k++) info->tune_ms[k] = J->tune_ms[k];
+  for (int k = 0; k < 4; k++) info->tune_ms[k] = J->tune_ms[k];
   return SGT_OK;
 }
 

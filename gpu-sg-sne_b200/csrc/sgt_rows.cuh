@@ -315,25 +315,6 @@ k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 }
 
 // ---------------------------------------------------------------------------
-// The same SpMV with the row tiles of the blocks that share an SM next to
-// each other.  Blocks are dispatched in index order over the SMs, so blocks
-// b, b + stripes, b + 2 stripes, ... (stripes = the SM count) run side by
-// side on one SM; here they take consecutive row tiles of one stripe of the
-// rows, and when the points are in a locality order their coordinate
-// gathers share that SM's L1.  Launched with stripes * ceil(tiles / stripes)
-// blocks; the blocks past the last tile have no rows.
-// ---------------------------------------------------------------------------
-template <int D, int G>
-__global__ void __launch_bounds__(SGT_THREADS, (D == 3 ? 6 : 8))
-k_attr_rows_swz(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
-                const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
-                int n, int row0, int stripes) {
-  const int q = (int)(gridDim.x / stripes);
-  const int tile = (int)(blockIdx.x % stripes) * q + (int)(blockIdx.x / stripes);
-  k_attr_rows_body<D, G>(tile, gridDim.x, rowptr, pairs, Y, Fattr, n, row0);
-}
-
-// ---------------------------------------------------------------------------
 // Attractive term only (operator entry points and the COO/ELL formats).
 // ---------------------------------------------------------------------------
 template <int D, int G>

@@ -3,28 +3,21 @@
 // Two native threads share the device with the caller:
 //   admission  takes waiting requests in FIFO order as soon as the request's
 //              footprint fits the HBM budget and a slot is free, builds its
-//              job (P upload, autotune, Y0) on a stream of its own and hands
-//              it to the scheduler with an event that marks it ready;
-//   scheduler  runs the small jobs (fewer than SGT_SERVE_SMALL points) in
-//              rounds: every one of them advances by the same number of
-//              iterations (at most `iters_per_round`, at most what any of
-//              them has left) through sgt_batch_step, which issues each
-//              stage of an iteration as one launch over all of them; their
-//              iterations are short and launch-bound alone.  Large jobs are
-//              throughput-bound alone: each runs its own captured iteration
-//              graphs on its own stream (stream priority rising as n falls),
-//              beside the rounds.  The scheduler keeps `rounds_ahead` rounds
-//              (and graph rounds per large job) queued, adds newly ready
-//              jobs, and when a job's last iteration has run, copies its
-//              coordinates to the caller's buffer, frees its memory
-//              (stream-ordered, no device synchronisation) and returns its
-//              footprint to the budget.
-// Jobs therefore share the GPU as soon as they are ready, whatever their
-// size or arrival time; a round costs about a dozen launches per iteration
-// however many small jobs it holds.
+//              job (P upload, autotune, Y0) on a stream of its own and queues
+//              the first round;
+//   scheduler  keeps every running job `rounds_ahead` rounds of
+//              `iters_per_round` iterations ahead of the GPU (one graph
+//              launch per round, an event per round), and when a job's last
+//              round has run copies its coordinates to the caller's buffer,
+//              frees its memory (stream-ordered, no device synchronisation)
+//              and returns its footprint to the budget.
+// Jobs therefore overlap on the GPU whatever their size or arrival time; the
+// hardware interleaves the kernels of all streams.  Streams carry priorities
+// that rise as n falls, so the short iterations of small embeddings are not
+// queued behind the thousands of blocks of a large one.
 //
-// Only the public C ABI of the engine is used (sgt_job_*, sgt_batch_step),
-// plus the CUDA runtime for streams and events.
+// Only the public C ABI of the engine is used (sgt_job_*), plus the CUDA
+// runtime for streams and events.
 #include "../../include/sgtsne_b200.h"
 
 #include <cuda_runtime.h>
@@ -59,18 +52,7 @@ struct Request {
   struct Slot *slot = nullptr;
   sgt_job *job = nullptr;
   int iters_total = 0, iters_queued = 0;
-  cudaEvent_t ready = nullptr;       // recorded on the slot's stream after set_y
-  std::deque<cudaEvent_t> inflight;  // a large job's queued graph rounds
-};
-
-// jobs of at least this many points run their own graphs beside the rounds
-constexpr int SGT_SERVE_SMALL = 65536;
-
-// a queued round: its completion event and the requests whose last
-// iteration it holds
-struct Round {
-  cudaEvent_t ev = nullptr;
-  std::vector<Request *> last;
+  std::deque<cudaEvent_t> inflight;  // one event per queued round
 };
 
 struct Slot {
@@ -102,8 +84,6 @@ struct sgt_server {
   bool stop = false;
 
   std::thread admit_thr, sched_thr;
-  sgt_ctx *rounds = nullptr;             // the context whose stream carries the rounds
-  cudaStream_t rounds_stream = nullptr;  // that stream
 
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -167,6 +147,26 @@ void finish_locked(sgt_server *srv, Request *r, int state, sgt_status status) {
   srv->cv_admit.notify_all();
 }
 
+sgt_status queue_round(Request *r, int iters_per_round, std::vector<cudaEvent_t> &pool) {
+  const int k = std::min(iters_per_round, r->iters_total - r->iters_queued);
+  sgt_status st = sgt_job_run(r->job, k);
+  if (st != SGT_OK) return st;
+  cudaEvent_t ev = nullptr;
+  if (!pool.empty()) {
+    ev = pool.back();
+    pool.pop_back();
+  } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    return SGT_ERR_CUDA;
+  }
+  if (cudaEventRecord(ev, r->slot->stream) != cudaSuccess) {
+    pool.push_back(ev);
+    return SGT_ERR_CUDA;
+  }
+  r->inflight.push_back(ev);
+  r->iters_queued += k;
+  return SGT_OK;
+}
+
 void admission_loop(sgt_server *srv) {
   cudaSetDevice(srv->device);
   std::vector<cudaEvent_t> pool;  // events created here move to the scheduler
@@ -206,25 +206,14 @@ void admission_loop(sgt_server *srv) {
       if (st == SGT_OK) st = sgt_job_set_y(job, r->y0, SGT_LAYOUT_POINT_MAJOR, 0);
       if (st == SGT_OK) {
         r->job = job;
-        if (pool.empty()) {
-          cudaEvent_t e = nullptr;
-          if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) st = SGT_ERR_CUDA;
-          else pool.push_back(e);
-        }
-        if (st == SGT_OK) {
-          r->ready = pool.back();
-          pool.pop_back();
-          if (cudaEventRecord(r->ready, slot->stream) != cudaSuccess) st = SGT_ERR_CUDA;
-        }
+        st = queue_round(r, srv->cfg.iters_per_round, pool);
       }
       if (st != SGT_OK && job) {
         cudaStreamSynchronize(slot->stream);
         sgt_job_destroy(job);
         r->job = nullptr;
-      }
-      if (st != SGT_OK && r->ready) {
-        cudaEventDestroy(r->ready);
-        r->ready = nullptr;
+        for (cudaEvent_t e : r->inflight) cudaEventDestroy(e);
+        r->inflight.clear();
       }
     }
     lk.lock();
@@ -241,155 +230,56 @@ void admission_loop(sgt_server *srv) {
   for (cudaEvent_t e : pool) cudaEventDestroy(e);
 }
 
-// a large job's next graph round on its own stream, with an event
-sgt_status queue_own_round(Request *r, int iters_per_round, std::vector<cudaEvent_t> &pool) {
-  const int k = std::min(iters_per_round, r->iters_total - r->iters_queued);
-  sgt_status st = sgt_job_run(r->job, k);
-  if (st != SGT_OK) return st;
-  cudaEvent_t ev = nullptr;
-  if (!pool.empty()) {
-    ev = pool.back();
-    pool.pop_back();
-  } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
-    return SGT_ERR_CUDA;
-  }
-  if (cudaEventRecord(ev, r->slot->stream) != cudaSuccess) {
-    pool.push_back(ev);
-    return SGT_ERR_CUDA;
-  }
-  r->inflight.push_back(ev);
-  r->iters_queued += k;
-  return SGT_OK;
-}
-
-// the request leaves: coordinates to the caller once `after` has run on the
-// rounds' stream, job freed on its own stream
-void retire(sgt_server *srv, Request *r, cudaEvent_t after, sgt_status st) {
-  if (after && cudaStreamWaitEvent(r->slot->stream, after, 0) != cudaSuccess) st = SGT_ERR_CUDA;
-  if (st == SGT_OK) st = sgt_job_get_y(r->job, r->y_out, SGT_LAYOUT_POINT_MAJOR, 0, 1);
-  cudaStreamSynchronize(r->slot->stream);
-  sgt_job_destroy(r->job);
-  r->job = nullptr;
-  std::lock_guard<std::mutex> lk(srv->mu);
-  finish_locked(srv, r, st == SGT_OK ? SGT_REQ_DONE : SGT_REQ_FAILED, st);
-}
-
 void scheduler_loop(sgt_server *srv) {
   cudaSetDevice(srv->device);
-  std::vector<Request *> running;  // small jobs with iterations left to queue
-  std::vector<Request *> large;    // large jobs, on their own streams
-  std::deque<Round> rounds;        // queued rounds, oldest first
+  std::vector<Request *> running;
   std::vector<cudaEvent_t> pool;
-  std::vector<sgt_job *> batch;
-  bool idle_stop = false;
   for (;;) {
-    std::vector<Request *> fresh;
     {
       std::unique_lock<std::mutex> lk(srv->mu);
-      if (running.empty() && rounds.empty() && large.empty())
+      if (running.empty())
         srv->cv_sched.wait(lk, [&] {
           return !srv->ready.empty() || (srv->stop && srv->active == 0);
         });
-      fresh.swap(srv->ready);
-      idle_stop = srv->stop && srv->active == 0;
+      running.insert(running.end(), srv->ready.begin(), srv->ready.end());
+      srv->ready.clear();
+      if (running.empty() && srv->stop && srv->active == 0) break;
     }
-    if (fresh.empty() && running.empty() && rounds.empty() && large.empty() && idle_stop) break;
-    bool progress = !fresh.empty();
-    for (Request *r : fresh) {
-      if (r->n >= SGT_SERVE_SMALL) {  // runs on its own stream, which holds its upload
-        pool.push_back(r->ready);
-        r->ready = nullptr;
-        large.push_back(r);
-        continue;
-      }
-      // the rounds' stream starts on the job once its upload and Y0 are done
-      if (cudaStreamWaitEvent(srv->rounds_stream, r->ready, 0) != cudaSuccess) {
-        retire(srv, r, nullptr, SGT_ERR_CUDA);
-        continue;
-      }
-      pool.push_back(r->ready);
-      r->ready = nullptr;
-      if (r->iters_total == 0) {
-        retire(srv, r, nullptr, SGT_OK);
-        continue;
-      }
-      running.push_back(r);
-    }
-    // large jobs: keep `rounds_ahead` graph rounds queued on each job's stream
-    for (size_t q = 0; q < large.size();) {
-      Request *r = large[q];
+    bool progress = false;
+    for (size_t k = 0; k < running.size();) {
+      Request *r = running[k];
       while (!r->inflight.empty() && cudaEventQuery(r->inflight.front()) == cudaSuccess) {
         pool.push_back(r->inflight.front());
         r->inflight.pop_front();
         progress = true;
       }
       sgt_status st = SGT_OK;
-      if (r->iters_queued < r->iters_total && (int)r->inflight.size() < srv->cfg.rounds_ahead) {
-        st = queue_own_round(r, srv->cfg.iters_per_round, pool);
+      if (r->iters_queued < r->iters_total &&
+          (int)r->inflight.size() < srv->cfg.rounds_ahead) {
+        st = queue_round(r, srv->cfg.iters_per_round, pool);
         progress = true;
       }
-      if (st != SGT_OK || (r->iters_queued == r->iters_total && r->inflight.empty())) {
+      const bool done = st == SGT_OK && r->iters_queued == r->iters_total && r->inflight.empty();
+      if (st != SGT_OK || done) {
+        if (done) st = sgt_job_get_y(r->job, r->y_out, SGT_LAYOUT_POINT_MAJOR, 0, 1);
+        cudaStreamSynchronize(r->slot->stream);
         for (cudaEvent_t e : r->inflight) pool.push_back(e);
         r->inflight.clear();
-        retire(srv, r, nullptr, st);
-        large.erase(large.begin() + q);
+        sgt_job_destroy(r->job);
+        r->job = nullptr;
+        {
+          std::lock_guard<std::mutex> lk(srv->mu);
+          finish_locked(srv, r, st == SGT_OK ? SGT_REQ_DONE : SGT_REQ_FAILED, st);
+        }
+        running.erase(running.begin() + k);
         progress = true;
         continue;
       }
-      q++;
-    }
-    // retire what the finished rounds completed
-    while (!rounds.empty() && cudaEventQuery(rounds.front().ev) == cudaSuccess) {
-      Round rd = rounds.front();
-      rounds.pop_front();
-      for (Request *r : rd.last) retire(srv, r, rd.ev, SGT_OK);
-      pool.push_back(rd.ev);
-      progress = true;
-    }
-    // queue the next round over every running job
-    if (!running.empty() && (int)rounds.size() < srv->cfg.rounds_ahead) {
-      int k = srv->cfg.iters_per_round;
-      for (Request *r : running) k = std::min(k, r->iters_total - r->iters_queued);
-      batch.clear();
-      for (Request *r : running) batch.push_back(r->job);
-      sgt_status st = sgt_batch_step(srv->rounds, (int)batch.size(), batch.data(), k);
-      Round rd;
-      if (st == SGT_OK) {
-        if (pool.empty()) {
-          cudaEvent_t e = nullptr;
-          if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) st = SGT_ERR_CUDA;
-          else pool.push_back(e);
-        }
-      }
-      if (st == SGT_OK) {
-        rd.ev = pool.back();
-        pool.pop_back();
-        if (cudaEventRecord(rd.ev, srv->rounds_stream) != cudaSuccess) st = SGT_ERR_CUDA;
-      }
-      if (st != SGT_OK) {
-        // the round failed: every running job fails once the queued work ran
-        cudaStreamSynchronize(srv->rounds_stream);
-        for (Request *r : running) retire(srv, r, nullptr, st);
-        running.clear();
-        if (rd.ev) pool.push_back(rd.ev);
-        continue;
-      }
-      for (size_t q = 0; q < running.size();) {
-        Request *r = running[q];
-        r->iters_queued += k;
-        if (r->iters_queued == r->iters_total) {
-          rd.last.push_back(r);
-          running.erase(running.begin() + q);
-        } else {
-          q++;
-        }
-      }
-      rounds.push_back(rd);
-      progress = true;
+      k++;
     }
     if (!progress) {
-      // every running job is `rounds_ahead` rounds ahead and no round has
-      // finished: wait a little, or until a new job is ready
+      // nothing finished and every job is `rounds_ahead` rounds ahead:
+      // wait a little, or until a new job is admitted
       std::unique_lock<std::mutex> lk(srv->mu);
       srv->cv_sched.wait_for(lk, std::chrono::microseconds(50),
                              [&] { return !srv->ready.empty(); });
@@ -433,19 +323,6 @@ sgt_status sgt_server_create(int device, const sgt_server_config *cfg, sgt_serve
   if (cudaDeviceGetStreamPriorityRange(&srv->prio_least, &srv->prio_greatest) != cudaSuccess) {
     srv->prio_least = srv->prio_greatest = 0;
   }
-  sgt_status cs = sgt_create(device, &srv->rounds);
-  // the rounds of small jobs get the greatest priority: short iterations
-  // should not queue behind the blocks of the large jobs' graphs
-  if (cs == SGT_OK && cudaStreamCreateWithPriority(&srv->rounds_stream, cudaStreamNonBlocking,
-                                                   srv->prio_greatest) != cudaSuccess)
-    cs = SGT_ERR_CUDA;
-  if (cs == SGT_OK) cs = sgt_set_stream(srv->rounds, srv->rounds_stream);
-  if (cs != SGT_OK) {
-    if (srv->rounds) sgt_destroy(srv->rounds);
-    if (srv->rounds_stream) cudaStreamDestroy(srv->rounds_stream);
-    delete srv;
-    return cs;
-  }
   srv->admit_thr = std::thread(admission_loop, srv);
   srv->sched_thr = std::thread(scheduler_loop, srv);
   *out = srv;
@@ -467,8 +344,6 @@ void sgt_server_destroy(sgt_server *srv) {
   }
   srv->sched_thr.join();
   cudaSetDevice(srv->device);
-  sgt_destroy(srv->rounds);
-  cudaStreamDestroy(srv->rounds_stream);
   for (auto &s : srv->slots) {
     sgt_destroy(s->ctx);
     cudaStreamDestroy(s->stream);
@@ -482,8 +357,7 @@ sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n, c
   if (!srv || !params || !rowptr || !col || !val || !y0 || !y_out || !id || n < 2)
     return SGT_ERR_INVALID_ARG;
   if (params->d < 1 || params->d > 3 || params->max_iter < 0) return SGT_ERR_UNSUPPORTED;
-  if (params->relayout_every > 0 || params->kl_every > 0 || params->format != SGT_FORMAT_CSR)
-    return SGT_ERR_UNSUPPORTED;
+  if (params->relayout_every > 0 || params->kl_every > 0) return SGT_ERR_UNSUPPORTED;
   std::unique_ptr<Request> r(new Request());
   r->p = *params;
   r->n = n;

@@ -55,8 +55,7 @@ class Params(C.Structure):
 class JobInfo(C.Structure):
     _fields_ = [("iter", C.c_int), ("grid_points", C.c_int), ("h_eff", C.c_float),
                 ("zeta", C.c_double), ("kl", C.c_double), ("error_flags", C.c_int),
-                ("nnz", C.c_long), ("row_group", C.c_int), ("row_order", C.c_int),
-                ("tune_ms", C.c_float * 8)]
+                ("nnz", C.c_long), ("row_group", C.c_int), ("tune_ms", C.c_float * 4)]
 
 
 class ServerConfig(C.Structure):
@@ -414,6 +413,12 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def batch_step(ctx: Context, jobs, iters: int):
+    """sgt_batch_step: `iters` fused iterations of `jobs` on ctx's stream."""
+    arr = (C.c_void_p * len(jobs))(*[j.h for j in jobs])
+    ctx.check(ctx.lib.sgt_batch_step(ctx.h, len(jobs), arr, int(iters)), "batch_step")
 
 
 def job_footprint(params: Params, n: int, nnz: int) -> int:

@@ -177,10 +177,7 @@ typedef struct {
   int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
   long nnz;          /* nonzeros of P                             */
   int row_group;     /* lanes per row picked by the autotuner      */
-  int row_order;     /* 1: the autotuner gave the blocks that share an
-                        SM neighbouring row tiles, 0: index order      */
-  float tune_ms[8];  /* row kernel ms measured for 4, 8, 16, 32 lanes,
-                        [0..3] index order, [4..7] neighbouring tiles */
+  float tune_ms[4];  /* row kernel ms measured for 4, 8, 16, 32 lanes */
 } sgt_job_info;
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
@@ -221,10 +218,10 @@ sgt_status sgt_batch_run(sgt_batch *batch, int iters);
 void sgt_batch_destroy(sgt_batch *batch);
 /* The same fused launches without a batch object or graph: queue `iters`
    iterations of the given jobs (CSR, no relayout or in-loop KL) on ctx's
-   stream, for a set of jobs that changes from call to call (the server's
-   rounds).  Jobs may belong to other contexts of the same device; their
-   streams must have finished the jobs' earlier work (the caller orders
-   them, e.g. with events). */
+   stream, for a set of jobs that changes from call to call.  Jobs may
+   belong to other contexts of the same device; their streams must have
+   finished the jobs' earlier work (the caller orders them, e.g. with
+   events). */
 sgt_status sgt_batch_step(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int iters);
 
 /* ---- one embedding split by rows over ranks (one GPU per rank) ---------
@@ -280,11 +277,10 @@ size_t sgt_job_footprint(const sgt_params *params, int n, long nnz);
  * priority rises as n falls, so short requests are not stuck behind long
  * ones).  An admission thread turns waiting requests into jobs, in FIFO
  * order, as soon as their footprint fits the budget and a slot is free; a
- * scheduler thread runs rounds in which every running job advances by up to
- * `iters_per_round` iterations through fused launches over all of them
- * (sgt_batch_step), keeps `rounds_ahead` rounds queued, adds jobs as they
- * become ready, copies a finished job's coordinates to the caller's buffer
- * and returns its memory to the budget.  Requests that arrive while others run
+ * scheduler thread keeps every running job `rounds_ahead` rounds of
+ * `iters_per_round` iterations ahead of the GPU (one graph launch per
+ * round), copies a finished job's coordinates to the caller's buffer and
+ * returns its memory to the budget.  Requests that arrive while others run
  * are admitted while those are still on the GPU; their kernels overlap. */
 typedef struct sgt_server sgt_server;
 typedef struct {
@@ -317,9 +313,7 @@ void sgt_server_destroy(sgt_server *srv);
    (as sgt_job_create); y0 and y_out: host, point-major n*d.  All caller-owned
    and kept alive until the request is done or failed.  params->max_iter is
    the number of iterations; the result is centred as after the reference's
-   last iteration.  params->format must be SGT_FORMAT_CSR (the rounds run
-   every job through the fused launches of sgt_batch_step), without
-   relayout or in-loop KL.  *id receives the request id (0, 1, 2, ...). */
+   last iteration.  *id receives the request id (0, 1, 2, ...). */
 sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n,
                              const int *rowptr, const int *col,
                              const float *val, const float *y0, float *y_out,

@@ -135,6 +135,30 @@ def test_batch_of_mixed_formats(problems):
     ctx.close()
 
 
+def test_batch_step_matches_alone(problems):
+    """sgt_batch_step: the fused launches without a batch object, over a set
+    of jobs that changes between calls (two jobs, then three)."""
+    import sgtsne_b200 as S
+    ctx = S.Context(0)
+    alone = [run_alone(S, ctx, p, SHORT) for p in problems[:3]]
+    jobs = []
+    for rp, col, val, d, y0 in problems[:3]:
+        j = S.Job(ctx, params(S, d, SHORT), rp, col, val, device_mem=False)
+        j.set_y(y0, S.LAYOUT_POINT_MAJOR, False)
+        jobs.append(j)
+    S.batch_step(ctx, jobs[:2], 1)
+    S.batch_step(ctx, jobs[2:], 1)
+    S.batch_step(ctx, jobs, SHORT - 1)
+    for j, ref in zip(jobs, alone):
+        out = np.empty_like(ref)
+        j.get_y(out, S.LAYOUT_POINT_MAJOR, False, 1)
+        assert j.info().iter == SHORT
+        assert rel(out, ref) <= TOL_Y
+    for j in jobs:
+        j.close()
+    ctx.close()
+
+
 def test_batch_rejects_foreign_and_relayout(problems):
     import sgtsne_b200 as S
     c1, c2 = S.Context(0), S.Context(0)
@@ -262,13 +286,7 @@ def test_one_dimensional_batch_and_server(problems):
         j.close()
     ctx.close()
     srv = S.Server(0, max_active=2, iters_per_round=4)
-    # the server runs requests in CSR (fused rounds); other formats are refused
-    rp, col, val, y0, _ = probs[1]
-    with pytest.raises(S.SgtError) as e:
-        srv.submit(par(S.FORMAT_COO, SHORT), rp, col, val, y0)
-    assert e.value.status == 4
-    outs = [srv.submit(par(S.FORMAT_CSR, SHORT), rp, col, val, y0)[1]
-            for rp, col, val, y0, _ in probs]
+    outs = [srv.submit(par(fmt, SHORT), rp, col, val, y0)[1] for rp, col, val, y0, fmt in probs]
     done = []
     for _ in range(300):
         done += srv.poll(wait_ms=50)
