@@ -379,6 +379,34 @@ def test_locality_order_is_transparent(torch, ctx, oracle, d):
 
 
 @pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("n", [3000, 150000])
+def test_csr_spmv_kernels_agree_with_coo(torch, ctx, oracle, d, n):
+    """Whichever CSR SpMV the autotuner picks (the plain row kernel or the
+    one with a shared-memory coordinate window, sgt_job_info.row_window),
+    two iterations match the COO path's (rel-L2 <= 1e-5)."""
+    import sgtsne_b200 as S
+    k = 10
+    rng = np.random.default_rng(n + d)
+    col = rng.integers(0, n - 1, (n, k))
+    col += col >= np.arange(n)[:, None]
+    rp = (np.arange(n + 1) * k).astype(np.int32)
+    srp, sc, sv = oracle.symmetrize(rp, col.reshape(-1).astype(np.int32), rng.random(n * k) + 0.1,
+                                    1.0 / (2 * n))
+    Y0 = (rng.standard_normal((n, d)) * 1e-2).astype(np.float32)
+    out, win = {}, None
+    for fmt in (S.FORMAT_CSR, S.FORMAT_COO):
+        job = S.Job(ctx, S.default_params(d=d, format=fmt), srp, sc, sv.astype(np.float32),
+                    device_mem=False)
+        if fmt == S.FORMAT_CSR:
+            win = job.info().row_window
+        job.set_y(Y0, S.LAYOUT_POINT_MAJOR, False)
+        job.run(2)
+        out[fmt] = job.get_y(np.empty((n, d), np.float32), S.LAYOUT_POINT_MAJOR, False, 1)
+        job.close()
+    assert rel(out[S.FORMAT_CSR], out[S.FORMAT_COO]) <= 1e-5, win
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
 def test_repulsive_error_probe(torch, ctx, oracle, d):
     """sgt_job_repulsive_error (the -f probe of CU/compute_error.cu:80-99):
     after one iteration from Y0 the job's repulsive force was computed at the
