@@ -514,7 +514,6 @@ def run_ours(args, rank, world, local, dist):
                        "p_source": p_source, "p_engine_vs_stored": p_match,
                        "grid_points_start": grid_start, "grid_points_end": info.grid_points,
                        "h_eff_end": round(info.h_eff, 5), "row_group": info.row_group,
-                       "row_window": info.row_window,
                        "relayout_every": args.relayout,
                        "row_group_tune_ms": [round(x, 4) for x in info.tune_ms],
                        "l2": "inputs larger than L2 (P >= 400 MB), no flush",
@@ -528,9 +527,7 @@ def run_ours(args, rank, world, local, dist):
                        "knn": "sgt_knn, exact: the tcgen05 tensor-core filter (50-D, k = 30) "
                               "re-ranked with the SIMT arithmetic",
                        "expanded_state": expanded},
-            "roofline": {"bound": "hbm",
-                         "kernel": "the CSR attractive SpMV (k_attr_rows_win when row_window "
-                                   "> 0, else k_attr_rows)",
+            "roofline": {"bound": "hbm", "kernel": "k_attr_rows (CSR attractive SpMV)",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_source": src,
                          "algorithmic_bytes_per_launch": alg,

@@ -96,11 +96,7 @@ struct sgt_job {
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
   std::vector<void *> allocs;
   double last_kl = 0.0;
-  // row kernel ms for G = 4, 8, 16, 32: one block per row tile ([0..3]) and
-  // a stretch of rows per CTA with a coordinate window in shared memory
-  // ([4..7], k_attr_rows_win)
-  float tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int win = 0;  // > 0: the SpMV is k_attr_rows_win with this many window points
+  float tune_ms[4] = {0, 0, 0, 0};  // row kernel ms for G = 4, 8, 16, 32
 };
 
 // ---------------------------------------------------------------------------
@@ -624,12 +620,8 @@ static sgt_status enqueue_attractive(sgt_job *J, cudaStream_t s) {
   const VT *Yc = (const VT *)(J->Ygather ? J->Ygather : J->Ynext);
   if (J->format == SGT_FORMAT_CSR) {
     const int nb = (int)(((long)n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (J->win > 0)
-      k_attr_rows_win<D, G><<<ctx->nsm, SGT_WIN_THREADS, sizeof(VT) * (size_t)J->win, s>>>(
-          J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n, J->win);
-    else
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
-                                                   J->row0);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, Yc, (VT *)J->Fattr, n,
+                                                 J->row0);
   } else {
     if (J->format == SGT_FORMAT_HYBRID) {
       k_attr_ell<D><<<J->nb_pts, SGT_THREADS, 0, s>>>(n, J->ell_w, J->ell_cols, J->ell_vals, Yc,
@@ -806,20 +798,15 @@ static sgt_status ensure_scratch(sgt_ctx *ctx, int n, int d, int grid_mode, int 
 // fastest of G = 4, 8, 16, 32 is kept.
 // ---------------------------------------------------------------------------
 template <int D, int G>
-static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1,
-                       int win) {
+static float time_spmv(sgt_job *J, const float *tY, float *tF, cudaEvent_t e0, cudaEvent_t e1) {
   typedef typename Vec<D>::T VT;
   cudaStream_t s = J->ctx->stream;
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {  // the first launch warms caches
     cudaEventRecord(e0, s);
     const int nb = (int)(((long)J->n * G + SGT_THREADS - 1) / SGT_THREADS);
-    if (win > 0)
-      k_attr_rows_win<D, G><<<J->ctx->nsm, SGT_WIN_THREADS, sizeof(VT) * (size_t)win, s>>>(
-          J->rowptr, J->pairs, (const VT *)tY, (VT *)tF, J->n, win);
-    else
-      k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY,
-                                                   (VT *)tF, J->n, J->row0);
+    k_attr_rows<D, G><<<nb, SGT_THREADS, 0, s>>>(J->rowptr, J->pairs, (const VT *)tY, (VT *)tF,
+                                                 J->n, J->row0);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -844,29 +831,11 @@ static sgt_status tune_group_d(sgt_job *J) {
   const float *tY = buf;  // zero coordinates: the gather pattern of P, finite values
   float *tF = buf + np;
   const int cand[4] = {4, 8, 16, 32};
-  float t[8];
-  t[0] = time_spmv<D, 4>(J, tY, tF, e0, e1, 0);
-  t[1] = time_spmv<D, 8>(J, tY, tF, e0, e1, 0);
-  t[2] = time_spmv<D, 16>(J, tY, tF, e0, e1, 0);
-  t[3] = time_spmv<D, 32>(J, tY, tF, e0, e1, 0);
-  // the windowed kernel: a whole job's rows index all its points (a shard
-  // gathers from every rank's points and keeps the plain kernel)
-  int win = 0;
-  for (int k = 4; k < 8; k++) t[k] = 1e30f;
-  if (J->row0 == 0 && J->n_gather == J->n) {
-    int optin = 0;
-    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    win = (optin - 1024) / (int)sizeof(typename Vec<D>::T);
-    const int bytes = win * (int)sizeof(typename Vec<D>::T);
-    CK(cudaFuncSetAttribute(k_attr_rows_win<D, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CK(cudaFuncSetAttribute(k_attr_rows_win<D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CK(cudaFuncSetAttribute(k_attr_rows_win<D, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CK(cudaFuncSetAttribute(k_attr_rows_win<D, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    t[4] = time_spmv<D, 4>(J, tY, tF, e0, e1, win);
-    t[5] = time_spmv<D, 8>(J, tY, tF, e0, e1, win);
-    t[6] = time_spmv<D, 16>(J, tY, tF, e0, e1, win);
-    t[7] = time_spmv<D, 32>(J, tY, tF, e0, e1, win);
-  }
+  float t[4];
+  t[0] = time_spmv<D, 4>(J, tY, tF, e0, e1);
+  t[1] = time_spmv<D, 8>(J, tY, tF, e0, e1);
+  t[2] = time_spmv<D, 16>(J, tY, tF, e0, e1);
+  t[3] = time_spmv<D, 32>(J, tY, tF, e0, e1);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -874,11 +843,10 @@ static sgt_status tune_group_d(sgt_job *J) {
   CK(e);
   CK(cudaGetLastError());
   int best = 0;
-  for (int k = 1; k < 8; k++)
+  for (int k = 1; k < 4; k++)
     if (t[k] < t[best]) best = k;
-  J->G = cand[best % 4];
-  J->win = best >= 4 ? win : 0;
-  for (int k = 0; k < 8; k++) J->tune_ms[k] = t[k] < 1e29f ? t[k] : 0.f;
+  J->G = cand[best];
+  for (int k = 0; k < 4; k++) J->tune_ms[k] = t[k];
   return SGT_OK;
 }
 
@@ -1292,12 +1260,6 @@ static bool is_attractive_kernel(const void *f) {
       (const void *)k_attr_rows<2, 16>, (const void *)k_attr_rows<2, 32>,
       (const void *)k_attr_rows<3, 4>, (const void *)k_attr_rows<3, 8>,
       (const void *)k_attr_rows<3, 16>, (const void *)k_attr_rows<3, 32>,
-      (const void *)k_attr_rows_win<1, 4>, (const void *)k_attr_rows_win<1, 8>,
-      (const void *)k_attr_rows_win<1, 16>, (const void *)k_attr_rows_win<1, 32>,
-      (const void *)k_attr_rows_win<2, 4>, (const void *)k_attr_rows_win<2, 8>,
-      (const void *)k_attr_rows_win<2, 16>, (const void *)k_attr_rows_win<2, 32>,
-      (const void *)k_attr_rows_win<3, 4>, (const void *)k_attr_rows_win<3, 8>,
-      (const void *)k_attr_rows_win<3, 16>, (const void *)k_attr_rows_win<3, 32>,
       (const void *)k_attr_ell<1>, (const void *)k_attr_ell<2>, (const void *)k_attr_ell<3>,
       (const void *)k_attr_coo<1>, (const void *)k_attr_coo<2>, (const void *)k_attr_coo<3>};
   for (const void *g : fs)
@@ -2203,8 +2165,7 @@ sgt_status sgt_job_get_info(sgt_job *J, sgt_job_info *info) {
   info->error_flags = J->st_host->error;
   info->nnz = J->nnz;
   info->row_group = J->G;
-  info->row_window = J->win;
-  for (int k = 0; k < 8; k++) info->tune_ms[k] = J->tune_ms[k];
+  for (int k = 0; k < 4; k++) info->tune_ms[k] = J->tune_ms[k];
   return SGT_OK;
 }
 

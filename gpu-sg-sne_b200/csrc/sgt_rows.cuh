@@ -315,76 +315,6 @@ k_attr_rows(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
 }
 
 // ---------------------------------------------------------------------------
-// The same SpMV with a window of coordinates in shared memory.  CTA c takes
-// the contiguous stretch of rows [c R, (c + 1) R) and first copies the
-// coordinates of the points win points around the stretch's middle into
-// shared memory with coalesced loads; a gather whose column falls in the
-// window reads shared memory, the others read global memory as k_attr_rows
-// does.  When the points are in a locality order (P's neighbours near each
-// other in memory) most of a stretch's gathers fall in its window, and a
-// gather served by shared memory sends no miss request from L1 to L2, the
-// request stream that bounds k_attr_rows.  Launched with one CTA per SM
-// (the window takes most of the shared memory), SGT_WIN_THREADS threads,
-// win * sizeof(Vec<D>) bytes of dynamic shared memory.
-// ---------------------------------------------------------------------------
-#define SGT_WIN_THREADS 1024
-
-template <int D, int G>
-__global__ void __launch_bounds__(SGT_WIN_THREADS, 1)
-k_attr_rows_win(const int *__restrict__ rowptr, const int2 *__restrict__ pairs,
-                const typename Vec<D>::T *__restrict__ Y, typename Vec<D>::T *__restrict__ Fattr,
-                int n, int win) {
-  typedef typename Vec<D>::T VT;
-  extern __shared__ __align__(16) unsigned char win_raw[];
-  VT *sY = reinterpret_cast<VT *>(win_raw);
-  const int R = (n + gridDim.x - 1) / gridDim.x;
-  const int r0 = blockIdx.x * R, r1 = min(n, r0 + R);
-  if (r0 >= r1) return;  // uniform over the block
-  const int w = min(win, n);
-  const int wlo = max(0, min(n - w, r0 + (r1 - r0) / 2 - w / 2));
-  for (int t = threadIdx.x; t < w; t += blockDim.x) sY[t] = __ldg(&Y[wlo + t]);
-  __syncthreads();
-  const int lane = threadIdx.x % G;
-  constexpr int GPB = SGT_WIN_THREADS / G;  // row groups per CTA
-  // uniform trip count over the block so the group shuffles stay converged
-  for (int base = r0; base < r1; base += GPB) {
-    const int i = base + threadIdx.x / G;
-    const bool valid = i < r1;
-    float acc[3] = {0.f, 0.f, 0.f};
-    if (valid) {
-      const int u = i - wlo;
-      const VT yi = (unsigned)u < (unsigned)w ? sY[u] : Y[i];
-      const int s = __ldcs(&rowptr[i]), e = __ldcs(&rowptr[i + 1]);
-      constexpr int U = 4;
-      for (int t0 = s + lane; t0 < e; t0 += U * G) {
-        int2 pr[U];
-#pragma unroll
-        for (int q = 0; q < U; q++) {
-          const int t = t0 + q * G;
-          pr[q] = t < e ? __ldcs(&pairs[t]) : make_int2(i, 0);
-        }
-        VT yj[U];
-#pragma unroll
-        for (int q = 0; q < U; q++) {
-          const int v = pr[q].x - wlo;
-          yj[q] = (unsigned)v < (unsigned)w ? sY[v] : __ldg(&Y[pr[q].x]);
-        }
-#pragma unroll
-        for (int q = 0; q < U; q++) attr_term<D>(yi, yj[q], __int_as_float(pr[q].y), acc);
-      }
-    }
-    group_reduce<D, G>(acc);
-    if (valid && lane == 0) {
-      VT f;
-      if constexpr (D == 3) f.w = 0.f;
-#pragma unroll
-      for (int k = 0; k < D; k++) setcomp<D>(f, k, acc[k]);
-      Fattr[i] = f;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Attractive term only (operator entry points and the COO/ELL formats).
 // ---------------------------------------------------------------------------
 template <int D, int G>

@@ -55,8 +55,7 @@ class Params(C.Structure):
 class JobInfo(C.Structure):
     _fields_ = [("iter", C.c_int), ("grid_points", C.c_int), ("h_eff", C.c_float),
                 ("zeta", C.c_double), ("kl", C.c_double), ("error_flags", C.c_int),
-                ("nnz", C.c_long), ("row_group", C.c_int), ("row_window", C.c_int),
-                ("tune_ms", C.c_float * 8)]
+                ("nnz", C.c_long), ("row_group", C.c_int), ("tune_ms", C.c_float * 4)]
 
 
 class ServerConfig(C.Structure):

@@ -177,11 +177,7 @@ typedef struct {
   int error_flags;   /* 1 non-finite, 2 grid clamped, 4 overflow  */
   long nnz;          /* nonzeros of P                             */
   int row_group;     /* lanes per row picked by the autotuner      */
-  int row_window;    /* > 0: the autotuner picked the SpMV that keeps
-                        this many coordinates around each CTA's stretch
-                        of rows in shared memory; 0: the plain one     */
-  float tune_ms[8];  /* row kernel ms measured for 4, 8, 16, 32 lanes,
-                        [0..3] plain, [4..7] with the window          */
+  float tune_ms[4];  /* row kernel ms measured for 4, 8, 16, 32 lanes */
 } sgt_job_info;
 sgt_status sgt_job_get_info(sgt_job *job, sgt_job_info *info);
 /* KL divergence of the current coordinates with the last Z (CU/pq.cu:104-125). */
