@@ -316,6 +316,7 @@ def run_params(S, args):
     p = S.default_params(d=2, format=S.FORMAT_CSR, max_iter=1000, early_iter=250, h=0.7)
     p.lambda_ = 10.0
     p.relayout_every = args.relayout
+    p.locality_order = args.locality_order
     return p
 
 
@@ -715,6 +716,8 @@ def main():
     ap.add_argument("--no-expanded", dest="expanded", action="store_false",
                     help="skip the fixed expanded-state (largest grid) line")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
+    ap.add_argument("--locality-order", type=int, default=1, choices=[0, 1],
+                    help="sgt_params.locality_order of every job (1: the engine default)")
     ap.add_argument("--knn-compare", type=int, default=200000,
                     help="points of the tensor-core vs SIMT kNN comparison (0 = skip)")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
@@ -727,6 +730,8 @@ def main():
     ap.add_argument("--serve-active", type=int, default=32)
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[2.0, 4.0])
     args = ap.parse_args()
+    from sgtsne_b200 import multi as _multi
+    _multi.LOCALITY_ORDER = args.locality_order
     rank, world, local = dist_env()
     import torch
     dist = dist_init(world, "nccl" if torch.cuda.is_available() else "gloo")

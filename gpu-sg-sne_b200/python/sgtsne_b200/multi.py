@@ -74,10 +74,16 @@ def request_instances(ctx, count, seed, dev, n_lo=1000, n_hi=500000, k=30):
     return out
 
 
+# sgt_params.locality_order of the jobs these helpers create (1: the
+# engine's default, a locality order of the points at creation)
+LOCALITY_ORDER = 1
+
+
 def job_params(S, d, iters, lam=1.0):
     p = S.default_params(d=d, format=S.FORMAT_CSR, max_iter=iters, early_iter=250,
                          h=0.7 if d == 2 else 1.2)
     p.lambda_ = lam
+    p.locality_order = LOCALITY_ORDER
     return p
 
 
