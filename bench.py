@@ -461,6 +461,12 @@ def run_ours(args, rank, world, local, dist):
     pe = run_params(S, args)
     pe.max_iter = 1000
     pe.lambda_dist = 1
+    # warm-up: one small call pages in the kernels of the preparation path
+    # (lambda bisection, symmetrisation, locality order) the run uses first
+    nw = 70000
+    pw = run_params(S, args)
+    pw.max_iter = 2
+    ctx.embed(e_rp.numpy()[:nw + 1], e_c.numpy()[:nw * k] % nw, e_v.numpy()[:nw * k], pw)
     barrier(dist, local)
     torch.cuda.synchronize()
     t0 = time.perf_counter()

@@ -34,6 +34,9 @@
 
 namespace {
 
+// requests of fewer points run without the locality order of job creation
+constexpr int SGT_SERVE_ORDER_MIN_N = 1000000;
+
 struct Request {
   long long id = 0;
   sgt_params p{};
@@ -360,6 +363,11 @@ sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n, c
   if (params->relayout_every > 0 || params->kl_every > 0) return SGT_ERR_UNSUPPORTED;
   std::unique_ptr<Request> r(new Request());
   r->p = *params;
+  // the locality order's creation cost (diffusion steps, relabelling) runs in
+  // the admission thread, under the load of the running jobs, and delays
+  // every admission behind it more than its faster SpMV gains over one
+  // request; it pays off for a single very large embedding only
+  if (n < SGT_SERVE_ORDER_MIN_N) r->p.locality_order = 0;
   r->n = n;
   r->nnz = rowptr[n];
   r->rowptr = rowptr;
@@ -368,7 +376,7 @@ sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n, c
   r->y0 = y0;
   r->y_out = y_out;
   r->iters_total = params->max_iter;
-  r->footprint = sgt_job_footprint(params, n, r->nnz);
+  r->footprint = sgt_job_footprint(&r->p, n, r->nnz);
   if (r->footprint == 0 || r->footprint > srv->cfg.hbm_budget) return SGT_ERR_NO_MEMORY;
   std::lock_guard<std::mutex> lk(srv->mu);
   if (srv->stop) return SGT_ERR_INVALID_ARG;

@@ -313,7 +313,10 @@ void sgt_server_destroy(sgt_server *srv);
    (as sgt_job_create); y0 and y_out: host, point-major n*d.  All caller-owned
    and kept alive until the request is done or failed.  params->max_iter is
    the number of iterations; the result is centred as after the reference's
-   last iteration.  *id receives the request id (0, 1, 2, ...). */
+   last iteration.  Requests of fewer than 1,000,000 points run without the
+   locality order of job creation (params->locality_order is ignored for
+   them): its cost lands in the admission of every later request.  *id
+   receives the request id (0, 1, 2, ...). */
 sgt_status sgt_server_submit(sgt_server *srv, const sgt_params *params, int n,
                              const int *rowptr, const int *col,
                              const float *val, const float *y0, float *y_out,
