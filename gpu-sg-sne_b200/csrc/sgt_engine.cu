@@ -2653,7 +2653,13 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
   CK(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
   const auto t0 = std::chrono::steady_clock::now();
-  CKS(check_csr(ctx, n, rowptr, col));
+  // rowptr on the host (the lambda bisection reads rows by it); the column
+  // indices are checked on the device by the symmetrisation, which rejects
+  // any outside [0, n) before anything reads through them
+  if (rowptr[0] != 0) return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr[0] != 0");
+  for (int i = 0; i < n; i++)
+    if (rowptr[i + 1] < rowptr[i])
+      return fail(ctx, SGT_ERR_INVALID_ARG, "rowptr not monotone at row " + std::to_string(i));
   const long nnz = rowptr[n];
   // P prepared on the device: lambda rescaling unless lambda == 1
   // (CU/sgtsne.cu:51-54), leaves dropped, (P + P^T)/(2n) (CU/sgtsne.cu:64-65)

@@ -324,6 +324,14 @@ def test_invalid_csr_rejected(torch, ctx):
     with pytest.raises(S.SgtError) as e:
         S.Job(ctx, p, rp, col, np.ones(3, np.float32), device_mem=False)
     assert e.value.status == 1
+    # sgt_embed: a column out of range is caught on the device, before the
+    # iterations; a non-monotone rowptr on the host
+    rp2 = np.array([0, 2, 3, 4], np.int32)
+    p.lambda_ = 3.0
+    for r, c in ((rp2, np.array([1, 2, 5, 0], np.int32)), (rp, col)):
+        with pytest.raises(S.SgtError) as e:
+            ctx.embed(r, c, np.ones(len(c), np.float32), p)
+        assert e.value.status == 1
 
 
 def test_relayout_is_transparent(torch, ctx):
