@@ -467,14 +467,19 @@ def run_ours(args, rank, world, local, dist):
     pw = run_params(S, args)
     pw.max_iter = 2
     ctx.embed(e_rp.numpy()[:nw + 1], e_c.numpy()[:nw * k] % nw, e_v.numpy()[:nw * k], pw)
-    barrier(dist, local)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ctx.embed(e_rp.numpy(), e_c.numpy(), e_v.numpy(), pe, y_in=y_in.numpy(),
-              y_out=y_out.numpy())
-    t1 = time.perf_counter()
-    barrier(dist, local)
-    e2e_s = max_over_ranks(dist, t1 - t0, dev)
+    # three whole calls; the line reports the median (one call is one
+    # embedding, and its wall time varies with the host)
+    walls = []
+    for _ in range(3):
+        barrier(dist, local)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.embed(e_rp.numpy(), e_c.numpy(), e_v.numpy(), pe, y_in=y_in.numpy(),
+                  y_out=y_out.numpy())
+        t1 = time.perf_counter()
+        barrier(dist, local)
+        walls.append(max_over_ranks(dist, t1 - t0, dev))
+    e2e_s = sorted(walls)[1]
     h2d = (e_rp.numel() * 4 + e_c.numel() * 4 + e_v.numel() * 4 + y_in.numel() * 4) / pe.max_iter
     d2h = y_out.numel() * 4 / pe.max_iter
     e2e = {"value": world * pe.max_iter / e2e_s, "unit": "iters/s",
@@ -482,7 +487,7 @@ def run_ours(args, rank, world, local, dist):
            "includes": "sgt_embed (the library entry) from pinned host buffers: the kNN graph "
                        "(k = 30 squared distances) in, lambda = 10 bisection, (P+P^T)/(2n), job "
                        "creation, the whole 1000-iteration run, the embedding back on the host",
-           "wall_s": e2e_s}
+           "wall_s": e2e_s, "wall_s_calls": [round(w, 4) for w in walls]}
     del e_rp, e_c, e_v
 
     batched = served = knn_cmp = None

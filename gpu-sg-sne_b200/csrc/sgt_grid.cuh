@@ -18,6 +18,46 @@
 #include "sgt_common.cuh"
 
 #define SGT_HIST_MAX 4096  // tiles held in shared memory by the binning kernels
+// Points a thread loads before it uses the first of them in the point loops
+// of the binning, S2G (cell mode) and G2S kernels: these kernels are bound by
+// load latency, not bandwidth, at a few warps per SM.
+#define SGT_PTS_U 4
+
+// Sums K per-lane values over the 32 lanes of a warp in K/2 + K/4 + ...
+// shuffles instead of 5K: at each step with offset O a lane keeps one half of
+// its values, sends the other half to lane ^ O and adds what it receives; once
+// the count no longer halves, the remaining offsets add whole vectors.  On
+// return acc[q], q < wsum_count(K, 16), of lane L holds the warp total of the
+// entry values acc[base + q], with base (zero on entry) advanced by the call;
+// lanes that share a base hold the same totals, and the lanes with
+// (L & wsum_full_mask(K, 16)) == 0 are one of each.
+__host__ __device__ constexpr int wsum_count(int k, int o) {
+  return o == 0 ? k : ((k % 2 == 0) ? wsum_count(k / 2, o / 2) : wsum_count(k, o / 2));
+}
+__host__ __device__ constexpr int wsum_full_mask(int k, int o) {
+  return o == 0 ? 0 : ((k % 2 == 0) ? wsum_full_mask(k / 2, o / 2) : (o | wsum_full_mask(k, o / 2)));
+}
+template <int K, int O>
+__device__ __forceinline__ void warp_multi_sum(float *acc, int lane, int &base) {
+  if constexpr (O > 0) {
+    if constexpr (K % 2 == 0) {
+      constexpr int H = K / 2;
+      const bool up = (lane & O) != 0;
+#pragma unroll
+      for (int q = 0; q < H; q++) {
+        const float send = up ? acc[q] : acc[q + H];
+        const float keep = up ? acc[q + H] : acc[q];
+        acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+      }
+      if (up) base += H;
+      warp_multi_sum<H, O / 2>(acc, lane, base);
+    } else {
+#pragma unroll
+      for (int q = 0; q < K; q++) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], O);
+      warp_multi_sum<K, O / 2>(acc, lane, base);
+    }
+  }
+}
 
 // Smallest FFT length >= need among 32, 64, 96, 128, 192, ..., 768, 1024
 // (2^k and 3 * 2^k): the 3 * 2^k lengths cut the padding of grids just above
@@ -218,28 +258,39 @@ __device__ __forceinline__ void k_bin_count_body(int vb_, int vg_, const typenam
   __syncthreads();
   // warp-uniform trip count: lanes with the same tile are merged with
   // match_any and add their count in one shared-memory atomic (points of an
-  // embedding cluster on few tiles)
+  // embedding cluster on few tiles).  A warp takes SGT_PTS_U runs of 32
+  // points per round and issues all their loads before the first use.
   const int lane = threadIdx.x & 31;
-  const long stride = (long)vg_ * blockDim.x;
-  for (long i0 = (long)vb_ * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
-    const int i = (int)i0 + lane;
-    int key = -1;
-    if (i < n) {
-      typename Vec<D>::T y = Ynext[i];
-      int f[3] = {0, 0, 0};
+  constexpr int U = SGT_PTS_U;
+  const long stride = (long)vg_ * blockDim.x * U;
+  for (long i0 = ((long)vb_ * blockDim.x + (threadIdx.x & ~31)) * U; i0 < n; i0 += stride) {
+    typename Vec<D>::T yv[U];
 #pragma unroll
-      for (int k = 0; k < D; k++) {
-        const float yc = __fsub_rn(comp<D>(y, k), mean[k]);
-        setcomp<D>(y, k, yc);
-        float sh;
-        const float s = sgt_scale(yc, miny[k], maxy, scale, sh);
-        f[k] = (int)floorf(s);
-      }
-      if (write_centred) Y[i] = y;
-      key = sgt_tile_of<D>(f, T, td);
+    for (int u = 0; u < U; u++) {
+      const long i = i0 + 32 * u + lane;
+      if (i < n) yv[u] = Ynext[i];
     }
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&hist[key], __popc(grp));
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long i = i0 + 32 * u + lane;
+      int key = -1;
+      if (i < n) {
+        typename Vec<D>::T y = yv[u];
+        int f[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+          const float yc = __fsub_rn(comp<D>(y, k), mean[k]);
+          setcomp<D>(y, k, yc);
+          float sh;
+          const float s = sgt_scale(yc, miny[k], maxy, scale, sh);
+          f[k] = (int)floorf(s);
+        }
+        if (write_centred) Y[i] = y;
+        key = sgt_tile_of<D>(f, T, td);
+      }
+      const unsigned grp = __match_any_sync(0xffffffffu, key);
+      if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&hist[key], __popc(grp));
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
@@ -359,51 +410,70 @@ __device__ __forceinline__ void k_bin_scatter_body(int vb_, int vg_, const typen
   __syncthreads();
   // warp-uniform trip counts; lanes of one tile are merged with match_any,
   // the group leader does the shared-memory atomic and the lanes take
-  // consecutive slots in lane order
+  // consecutive slots in lane order.  A warp takes SGT_PTS_U runs of 32
+  // points per round and issues all their loads before the first use.
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
-  for (int i0 = lo + (threadIdx.x & ~31); i0 < hi; i0 += blockDim.x) {
-    const int i = i0 + lane;
-    int key = -1;
-    if (i < hi) {
-      const typename Vec<D>::T y = Y[i];
-      int f[3] = {0, 0, 0};
+  constexpr int U = SGT_PTS_U;
+  const int wstart = lo + (threadIdx.x & ~31) * U, wstep = blockDim.x * U;
+  for (int i0 = wstart; i0 < hi; i0 += wstep) {
+    typename Vec<D>::T yv[U];
 #pragma unroll
-      for (int k = 0; k < D; k++) {
-        float sh;
-        f[k] = (int)floorf(sgt_scale(comp<D>(y, k), miny[k], maxy, scale, sh));
-      }
-      key = sgt_tile_of<D>(f, T, td);
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + 32 * u + lane;
+      if (i < hi) yv[u] = Y[i];
     }
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&lc[key], __popc(grp));
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + 32 * u + lane;
+      int key = -1;
+      if (i < hi) {
+        int f[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+          float sh;
+          f[k] = (int)floorf(sgt_scale(comp<D>(yv[u], k), miny[k], maxy, scale, sh));
+        }
+        key = sgt_tile_of<D>(f, T, td);
+      }
+      const unsigned grp = __match_any_sync(0xffffffffu, key);
+      if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&lc[key], __popc(grp));
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
     if (lc[t]) lc[t] = atomicAdd(&cursor[t], lc[t]);
   __syncthreads();
-  for (int i0 = lo + (threadIdx.x & ~31); i0 < hi; i0 += blockDim.x) {
-    const int i = i0 + lane;
-    int key = -1;
-    float4 rec = make_float4(0.f, 0.f, 0.f, __int_as_float(i));
-    if (i < hi) {
-      const typename Vec<D>::T y = Y[i];
-      int f[3] = {0, 0, 0};
+  for (int i0 = wstart; i0 < hi; i0 += wstep) {
+    typename Vec<D>::T yv[U];
 #pragma unroll
-      for (int k = 0; k < D; k++) {
-        float sh;
-        const float v = comp<D>(y, k);
-        f[k] = (int)floorf(sgt_scale(v, miny[k], maxy, scale, sh));
-        if (k == 0) rec.x = v; else if (k == 1) rec.y = v; else rec.z = v;
-      }
-      key = sgt_tile_of<D>(f, T, td);
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + 32 * u + lane;
+      if (i < hi) yv[u] = Y[i];
     }
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(grp) - 1;
-    int base = 0;
-    if (key >= 0 && lane == leader) base = atomicAdd(&lc[key], __popc(grp));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (key >= 0) sorted[base + __popc(grp & below)] = rec;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + 32 * u + lane;
+      int key = -1;
+      float4 rec = make_float4(0.f, 0.f, 0.f, __int_as_float(i));
+      if (i < hi) {
+        int f[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+          float sh;
+          const float v = comp<D>(yv[u], k);
+          f[k] = (int)floorf(sgt_scale(v, miny[k], maxy, scale, sh));
+          if (k == 0) rec.x = v; else if (k == 1) rec.y = v; else rec.z = v;
+        }
+        key = sgt_tile_of<D>(f, T, td);
+      }
+      const unsigned grp = __match_any_sync(0xffffffffu, key);
+      const int leader = __ffs(grp) - 1;
+      int base = 0;
+      if (key >= 0 && lane == leader) base = atomicAdd(&lc[key], __popc(grp));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (key >= 0) sorted[base + __popc(grp & below)] = rec;
+    }
   }
 }
 template <int D>
@@ -625,39 +695,54 @@ __device__ __forceinline__ void k_s2g_cell_body(int vb_, int vg_, const float4 *
       float acc[K];
 #pragma unroll
       for (int q = 0; q < K; q++) acc[q] = 0.f;
-      for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
-        const float4 rec = sorted[j];
-        int f[3];
-        float w[3][4], ys[3];
-        sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
-        bool ok = f[0] == cf[0];
-        if (D >= 2) ok = ok && f[1] == cf[1];
-        if (D >= 3) ok = ok && f[2] == cf[2];
-        if (!ok) {  // the sort and the binning disagree: skip the point
-          atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);
-          continue;
+      constexpr int U = SGT_PTS_U;
+      const int end = ch.y + ch.z;
+      for (int j0 = ch.y + threadIdx.x; j0 < end; j0 += U * blockDim.x) {
+        float4 rv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int j = j0 + u * blockDim.x;
+          if (j < end) rv[u] = sorted[j];
         }
-        float qc[3];
 #pragma unroll
-        for (int k = 0; k < D; k++) qc[k] = ys[k] - hc;
-        const float wz = D == 3 ? w[2][pass] : 1.f;
+        for (int u = 0; u < U; u++) {
+          if (j0 + u * blockDim.x >= end) break;
+          int f[3];
+          float w[3][4], ys[3];
+          sgt_point_stencil<D>(rv[u], miny, maxy, scale, f, w, ys);
+          bool ok = f[0] == cf[0];
+          if (D >= 2) ok = ok && f[1] == cf[1];
+          if (D >= 3) ok = ok && f[2] == cf[2];
+          if (!ok) {  // the sort and the binning disagree: skip the point
+            atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);
+            continue;
+          }
+          float qc[3];
 #pragma unroll
-        for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
-          const float wy = (D >= 2 ? w[1][a1] : 1.f) * wz;
+          for (int k = 0; k < D; k++) qc[k] = ys[k] - hc;
+          const float wz = D == 3 ? w[2][pass] : 1.f;
 #pragma unroll
-          for (int a0 = 0; a0 < 4; a0++) {
-            const float wt = wy * w[0][a0];
-            const int nd = a1 * 4 + a0;
-            acc[nd * C] += wt;
+          for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
+            const float wy = (D >= 2 ? w[1][a1] : 1.f) * wz;
 #pragma unroll
-            for (int k = 0; k < D; k++) acc[nd * C + 1 + k] += wt * qc[k];
+            for (int a0 = 0; a0 < 4; a0++) {
+              const float wt = wy * w[0][a0];
+              const int nd = a1 * 4 + a0;
+              acc[nd * C] += wt;
+#pragma unroll
+              for (int k = 0; k < D; k++) acc[nd * C + 1 + k] += wt * qc[k];
+            }
           }
         }
       }
+      {
+        int base = 0;
+        warp_multi_sum<K, 16>(acc, lane, base);
+        constexpr int KF = wsum_count(K, 16);
+        if ((lane & wsum_full_mask(K, 16)) == 0) {
 #pragma unroll
-      for (int q = 0; q < K; q++) {
-        const float v = warp_sum_f(acc[q]);
-        if (lane == 0) red[wid][q] = v;
+          for (int q = 0; q < KF; q++) red[wid][base + q] = acc[q];
+        }
       }
       __syncthreads();
       for (int q = threadIdx.x; q < K; q += blockDim.x) {
@@ -681,6 +766,40 @@ k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
   k_s2g_cell_body<D>(blockIdx.x, gridDim.x, sorted, st, chunks, V);
 }
 
+// Interpolated potentials p[0..d] at a point with stencil weights w and base
+// cell f: from the grid Phi, or (SM) from the block's copy cn of the 4^d nodes
+// of the point's cell, node a0 + 4 a1 + 16 a2.  Same products in the same
+// order either way.
+template <int D, bool SM>
+__device__ __forceinline__ void g2s_potentials(const float (*w)[4], const int *f, int N,
+                                               const typename Node<D>::T *__restrict__ Phi,
+                                               const typename Node<D>::T *cn, float *p) {
+#pragma unroll
+  for (int a2 = 0; a2 < (D >= 3 ? 4 : 1); a2++)
+#pragma unroll
+    for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
+      float wy = 1.f;
+      if (D >= 2) wy *= w[1][a1];
+      if (D >= 3) wy *= w[2][a2];
+      long base = f[0];
+      if (D >= 2) base += (long)N * (f[1] + a1);
+      if (D >= 3) base += (long)N * N * (f[2] + a2);
+#pragma unroll
+      for (int a0 = 0; a0 < 4; a0++) {
+        const float wt = wy * w[0][a0];
+        typename Node<D>::T v;
+        if constexpr (SM) v = cn[a0 + 4 * (a1 + 4 * a2)];
+        else v = __ldg(&Phi[base + a0]);
+        p[0] += wt * v.x;
+        p[1] += wt * v.y;
+        if constexpr (D >= 2) {
+          p[2] += wt * v.z;
+          if constexpr (D >= 3) p[3] += wt * v.w;
+        }
+      }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // G2S over chunks + repulsive force numerator + Z (FP64, fixed-order finish).
 // Frep_un[i] = y_i*Phi0 - Phi_{1..d}; Z = sum_i z_i - n.
@@ -698,48 +817,63 @@ __device__ __forceinline__ void k_g2s_body(int vb_, int vg_, const float4 *__res
   float miny[3];
 #pragma unroll
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  // cell mode (T = 1): every point of a chunk reads the same 4^d nodes,
+  // which the block stages once per chunk in shared memory
+  constexpr int NNODES = D == 1 ? 4 : (D == 2 ? 16 : 64);
+  __shared__ typename Node<D>::T cn[NNODES];
+  const bool cell = st->T == 1;
+  const int td = st->tiles_dim;
   double zacc = 0.0;
   for (int c = vb_; c < nch; c += vg_) {
     const int4 ch = chunks[c];
-    for (int j = ch.y + threadIdx.x; j < ch.y + ch.z; j += blockDim.x) {
-      const float4 rec = sorted[j];
-      int f[3];
-      float w[3][4], ys[3];
-      sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
-      float p[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-      for (int a2 = 0; a2 < (D >= 3 ? 4 : 1); a2++)
-#pragma unroll
-        for (int a1 = 0; a1 < (D >= 2 ? 4 : 1); a1++) {
-          float wy = 1.f;
-          if (D >= 2) wy *= w[1][a1];
-          if (D >= 3) wy *= w[2][a2];
-          long base = f[0];
-          if (D >= 2) base += (long)N * (f[1] + a1);
-          if (D >= 3) base += (long)N * N * (f[2] + a2);
-#pragma unroll
-          for (int a0 = 0; a0 < 4; a0++) {
-            const float wt = wy * w[0][a0];
-            const typename Node<D>::T v = __ldg(&Phi[base + a0]);
-            p[0] += wt * v.x;
-            p[1] += wt * v.y;
-            if constexpr (D >= 2) {
-              p[2] += wt * v.z;
-              if constexpr (D >= 3) p[3] += wt * v.w;
-            }
-          }
-        }
-      double ysq = 0.0, dot = 0.0;
-      typename Vec<D>::T fr;
-#pragma unroll
-      for (int k = 0; k < D; k++) {
-        const float yk = ys[k] - hc;
-        ysq += (double)yk * yk;
-        dot += (double)yk * p[k + 1];
-        setcomp<D>(fr, k, yk * p[0] - p[k + 1]);
+    int cf[3] = {-1, -1, -1};
+    if (cell) {  // block-uniform
+      cf[0] = ch.x % td;
+      if (D >= 2) cf[1] = (ch.x / td) % td;
+      if (D >= 3) cf[2] = ch.x / (td * td);
+      __syncthreads();  // the previous chunk's points are done with cn
+      for (int e = threadIdx.x; e < NNODES; e += blockDim.x) {
+        long g = cf[0] + (e & 3);
+        if (D >= 2) g += (long)N * (cf[1] + ((e >> 2) & 3));
+        if (D >= 3) g += (long)N * N * (cf[2] + (e >> 4));
+        cn[e] = Phi[g];
       }
-      zacc += (1.0 + 2.0 * ysq) * (double)p[0] - 2.0 * dot;
-      Frep_un[__float_as_int(rec.w)] = fr;
+      __syncthreads();
+    }
+    constexpr int U = SGT_PTS_U;
+    const int end = ch.y + ch.z;
+    for (int j0 = ch.y + threadIdx.x; j0 < end; j0 += U * blockDim.x) {
+      float4 rv[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int j = j0 + u * blockDim.x;
+        if (j < end) rv[u] = sorted[j];
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (j0 + u * blockDim.x >= end) break;
+        const float4 rec = rv[u];
+        int f[3];
+        float w[3][4], ys[3];
+        sgt_point_stencil<D>(rec, miny, maxy, scale, f, w, ys);
+        bool here = cell && f[0] == cf[0];
+        if (D >= 2) here = here && f[1] == cf[1];
+        if (D >= 3) here = here && f[2] == cf[2];
+        float p[4] = {0.f, 0.f, 0.f, 0.f};
+        if (here) g2s_potentials<D, true>(w, f, N, Phi, cn, p);
+        else g2s_potentials<D, false>(w, f, N, Phi, cn, p);
+        double ysq = 0.0, dot = 0.0;
+        typename Vec<D>::T fr;
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+          const float yk = ys[k] - hc;
+          ysq += (double)yk * yk;
+          dot += (double)yk * p[k + 1];
+          setcomp<D>(fr, k, yk * p[0] - p[k + 1]);
+        }
+        zacc += (1.0 + 2.0 * ysq) * (double)p[0] - 2.0 * dot;
+        Frep_un[__float_as_int(rec.w)] = fr;
+      }
     }
   }
   zacc = warp_sum_d(zacc);
