@@ -504,8 +504,9 @@ def run_ours(args, rank, world, local, dist):
         hbm, src = peaks()
         achieved = alg / (spmv_ms / 1e3) / 1e9
         ratio = read_traffic(nnz, n)
-        # bin count/scan/scatter, s2g (tile + cell), fft x3, g2s, SpMV, combine
-        per_iter_kernels = 11
+        # bin count (with the tile scan in its last block), bin scatter,
+        # s2g (tile + cell), fft x3, g2s, SpMV, combine
+        per_iter_kernels = 10
         # a relayout before every R-th iteration: cell keys, two 3-kernel
         # scans, key scatter, permutation prep, row relabel, 3 gathers
         R = args.relayout

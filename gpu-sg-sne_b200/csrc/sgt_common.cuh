@@ -69,6 +69,7 @@ struct SgtState {
   unsigned int done_row;
   unsigned int done_kl;
   unsigned int done_init;
+  unsigned int done_bin;
   double kl;
   int error;
 };
@@ -123,6 +124,16 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Programmatic dependent launch.  The kernels of the repulsion chain after
+// the first are launched with programmatic stream serialisation, so the
+// hardware stages a kernel's launch while its predecessor on the stream
+// drains; every such kernel begins here, which waits until the predecessor
+// has completed and its writes are visible.  Launched without the attribute
+// (batches, the operator entry points, stage timing) the wait returns at once.
+__device__ __forceinline__ void sgt_pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ float warp_sum_f(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

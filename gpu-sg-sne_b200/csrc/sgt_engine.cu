@@ -44,7 +44,14 @@ struct sgt_ctx {
   void *step_tables = nullptr;
   size_t step_bytes = 0;
   cudaEvent_t step_ev[9] = {};
+  // the context's memory pool (release threshold: never), trimmed by
+  // sgt_destroy
+  cudaMemPool_t pool = nullptr;
 };
+
+cudaError_t sgti_alloc(sgt_ctx *ctx, void **p, size_t bytes, cudaStream_t s) {
+  return cudaMallocFromPoolAsync(p, bytes, ctx->pool, s);
+}
 
 struct sgt_job {
   sgt_ctx *ctx = nullptr;
@@ -87,7 +94,7 @@ struct sgt_job {
   double *part_sum = nullptr, *part_z = nullptr, *part_kl = nullptr;
   SgtState *st = nullptr;
   SgtState *st_host = nullptr;
-  int nb_pts = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0,
+  int nb_pts = 0, nb_bin = 0, nb_s2g = 0, nb_s2gc = 0, nb_g2s = 0, nb_fft = 0, nb_fft_rows = 0, nb_row = 0,
       nb_upd = 0, nb_part = 0;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // the two branches of an iteration
   size_t smem_s2g = 0, smem_s2g8 = 0, smem_fft1 = 0, smem_fft2 = 0;
@@ -139,9 +146,9 @@ sgt_status sgti_fail(sgt_ctx *ctx, sgt_status s, const std::string &msg) { retur
     if (s_ != SGT_OK) return s_;                                              \
   } while (0)
 
-// Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
-// context's stream from the device's default pool): creating or retiring a
-// job never waits for work on other streams, which cudaFree would (it
+// Device memory is stream-ordered (cudaMallocFromPoolAsync / cudaFreeAsync on
+// the context's stream from the context's pool): creating or retiring a job
+// never waits for work on other streams, which cudaFree would (it
 // synchronises the device).  Jobs of one context share its stream, so
 // every use of a buffer is ordered between its allocation and its free.
 template <typename T>
@@ -149,7 +156,7 @@ static sgt_status jalloc(sgt_job *J, T **ptr, size_t count) {
   sgt_ctx *ctx = J->ctx;
   void *p = nullptr;
   if (count == 0) count = 1;
-  CK(cudaMallocAsync(&p, count * sizeof(T), ctx->stream));
+  CK(sgti_alloc(ctx, (void **)&p, count * sizeof(T), ctx->stream));
   J->allocs.push_back(p);
   *ptr = (T *)p;
   return SGT_OK;
@@ -159,6 +166,8 @@ static int grid_blocks(int nsm, int per_sm) { return std::max(1, nsm * std::max(
 
 // iterations per launch of a job's chained graph (sgt_job_run)
 #define SGT_GRAPH_ITERS 16
+// nonzeros of P from which a job's repulsion chain runs one block per SM
+#define SGT_CHAIN_NARROW_NNZ 16000000L
 
 static void drop_graphs(sgt_job *J) {
   if (J->gexec) cudaGraphExecDestroy(J->gexec);
@@ -236,7 +245,20 @@ sgt_status sgt_create(int device, sgt_ctx **out) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    e = cudaMemPoolCreate(&ctx->pool, &props);
+    if (e == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   if (e != cudaSuccess) {
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SGT_ERR_CUDA;
@@ -258,6 +280,13 @@ void sgt_destroy(sgt_ctx *ctx) {
   }
   for (cudaEvent_t e : ctx->step_ev)
     if (e) cudaEventDestroy(e);
+  if (ctx->pool) {
+    // buffers still allocated (a job the caller did not destroy) keep the
+    // pool alive until they are freed
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->pool, 0);
+    cudaMemPoolDestroy(ctx->pool);
+  }
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   delete ctx;
@@ -337,7 +366,7 @@ static sgt_status hybrid_split_device(sgt_ctx *ctx, int n, const std::vector<int
   std::vector<long> tail((size_t)n + 1, 0);
   for (int r = 0; r < n; r++) tail[r + 1] = tail[r] + std::max(0, hrp[r + 1] - hrp[r] - w);
   long *dt = nullptr;
-  CK(cudaMallocAsync(&dt, sizeof(long) * ((size_t)n + 1), s));
+  CK(sgti_alloc(ctx, (void **)&dt, sizeof(long) * ((size_t)n + 1), s));
   cudaError_t e = cudaMemcpyAsync(dt, tail.data(), sizeof(long) * ((size_t)n + 1),
                                   cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
@@ -386,7 +415,7 @@ static sgt_status job_shapes(sgt_job *J) {
   J->nb_g2s = grid_blocks(nsm, occ);
   const int M = J->mmax;
   J->smem_fft1 = 0;
-  J->smem_fft2 = fft_cols_smem(M);
+  J->smem_fft2 = fft_cols_smem(M, D);
   if constexpr (D == 1) {
     J->nb_fft = 1;
   } else {
@@ -410,10 +439,24 @@ static sgt_status job_shapes(sgt_job *J) {
   J->nb_row = grid_blocks(nsm, occ);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_update<D, 1, false>, SGT_THREADS, 0));
   J->nb_upd = grid_blocks(nsm, occ);
+  // A job whose SpMV is large runs its repulsion chain beside an SpMV that
+  // holds every SM: a chain kernel's blocks start only as SpMV blocks retire,
+  // so one block per SM (each with more points) finishes sooner than four.
+  // 1.3M points (67M nonzeros): 337 against 351 us per iteration; 400k
+  // (20M): 114 against 119.
+  J->nb_bin = J->nb_pts;
+  if (J->nnz >= SGT_CHAIN_NARROW_NNZ) {
+    J->nb_bin = std::min(J->nb_bin, nsm);
+    J->nb_s2g = std::min(J->nb_s2g, nsm);
+    J->nb_s2g8 = std::min(J->nb_s2g8, nsm);
+    J->nb_s2gc = std::min(J->nb_s2gc, nsm);
+    J->nb_g2s = std::min(J->nb_g2s, nsm);
+  }
   // small embeddings launch no more blocks than there is work for: idle
   // blocks only take scheduling slots from the jobs that share the GPU
   const int cap = (int)std::max(1L, ((long)J->n + 255) / 256);
   J->nb_pts = std::min(J->nb_pts, cap);
+  J->nb_bin = std::min(J->nb_bin, cap);
   J->nb_s2g = std::min(J->nb_s2g, cap);
   J->nb_s2g8 = std::min(J->nb_s2g8, cap);
   J->nb_s2gc = std::min(J->nb_s2gc, cap);
@@ -528,19 +571,47 @@ static sgt_status job_new(sgt_ctx *ctx, const sgt_params *p, int n, sgt_job **ou
 // ---------------------------------------------------------------------------
 // iteration enqueue
 // ---------------------------------------------------------------------------
+// A kernel of the repulsion chain after its first: with pdl set, launched
+// with programmatic stream serialisation, so its launch is staged while its
+// predecessor on the stream drains (the kernel waits in sgt_pdl_wait before
+// it reads anything).  Stage timing passes pdl = false, so that the events
+// between the stages see whole kernels.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_chain(bool pdl, void (*k)(KArgs...), int grid, int block, size_t smem,
+                                cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <int D>
-static sgt_status enqueue_g2g(sgt_job *J, cudaStream_t s) {
+static sgt_status enqueue_g2g(sgt_job *J, cudaStream_t s, bool pdl) {
+  sgt_ctx *ctx = J->ctx;
   typedef typename Node<D>::T NT;
   if constexpr (D == 1) {
-    k_conv1d<<<1, 32, 0, s>>>(J->st, (const float2 *)J->V, (float2 *)J->Phi);
+    CK(launch_chain(pdl, k_conv1d, 1, 32, 0, s, (const SgtState *)J->st, (const float2 *)J->V,
+                    (float2 *)J->Phi));
   } else {
-    k_fft_build_x<D><<<J->nb_fft_rows, SGT_THREADS, 0, s>>>(J->st, (const NT *)J->V, J->W);
+    CK(launch_chain(pdl, k_fft_build_x<D>, J->nb_fft_rows, SGT_THREADS, 0, s,
+                    (const SgtState *)J->st, (const NT *)J->V, J->W));
     if constexpr (D == 3)
-      k_fft_cols<D, MODE_MID_FWD><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
-    k_fft_cols<D, MODE_LAST><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
+      CK(launch_chain(pdl, k_fft_cols<D, MODE_MID_FWD>, J->nb_fft, SGT_THREADS, J->smem_fft2, s,
+                      (const SgtState *)J->st, J->W, (const NT *)J->V, (NT *)J->Phi));
+    CK(launch_chain(pdl, k_fft_cols<D, MODE_LAST>, J->nb_fft, SGT_THREADS, J->smem_fft2, s,
+                    (const SgtState *)J->st, J->W, (const NT *)J->V, (NT *)J->Phi));
     if constexpr (D == 3)
-      k_fft_cols<D, MODE_MID_INV><<<J->nb_fft, SGT_THREADS, J->smem_fft2, s>>>(J->st, J->W);
-    k_fft_final_x<D><<<J->nb_fft_rows, SGT_THREADS, 0, s>>>(J->st, J->W, (NT *)J->Phi);
+      CK(launch_chain(pdl, k_fft_cols<D, MODE_MID_INV>, J->nb_fft, SGT_THREADS, J->smem_fft2, s,
+                      (const SgtState *)J->st, J->W, (const NT *)J->V, (NT *)J->Phi));
+    CK(launch_chain(pdl, k_fft_final_x<D>, J->nb_fft_rows, SGT_THREADS, 0, s,
+                    (const SgtState *)J->st, (const float2 *)J->W, (NT *)J->Phi));
   }
   return SGT_OK;
 }
@@ -551,8 +622,9 @@ static sgt_status enqueue_bin_count(sgt_job *J, cudaStream_t s) {
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   typedef typename Node<D>::T NT;
-  k_bin_count<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n,
-                                                   J->st, J->tile_count, (NT *)J->V, 1);
+  k_bin_count<D><<<J->nb_bin, SGT_THREADS, 0, s>>>((const VT *)J->Ynext, (VT *)J->Y, J->n,
+                                                   J->st, J->tile_count, (NT *)J->V, 1, J->jp,
+                                                   J->cursor, J->chunks, J->nb_s2g);
   CK(cudaGetLastError());
   return SGT_OK;
 }
@@ -565,16 +637,19 @@ static sgt_status enqueue_scatter_part(sgt_job *J, cudaStream_t s, cudaEvent_t *
   typedef typename Vec<D>::T VT;
   typedef typename Node<D>::T NT;
   const int n = J->n;
-  k_bin_scan<<<1, 1024, 0, s>>>(J->st, J->jp, J->tile_count, J->cursor, J->chunks, J->nb_s2g);
-  k_bin_scatter<D><<<J->nb_pts, SGT_THREADS, 0, s>>>((const VT *)J->Y, n, J->st, J->cursor,
-                                                     J->sorted);
+  const bool pdl = ev == nullptr;
+  CK(launch_chain(pdl, k_bin_scatter<D>, J->nb_bin, SGT_THREADS, 0, s, (const VT *)J->Y, n, J->st,
+                  J->cursor, J->sorted));
   if (ev) CK(cudaEventRecord(ev[1], s));
   // tile mode and cell mode: the kernel of the other mode returns at once
   constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
-  k_s2g<D, TT><<<J->nb_s2g, SGT_THREADS, J->smem_s2g, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+  CK(launch_chain(pdl, k_s2g<D, TT>, J->nb_s2g, SGT_THREADS, J->smem_s2g, s,
+                  (const float4 *)J->sorted, J->st, (const int4 *)J->chunks, (NT *)J->V));
   if constexpr (D == 3)
-    k_s2g<3, 8><<<J->nb_s2g8, SGT_THREADS, J->smem_s2g8, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
-  k_s2g_cell<D><<<J->nb_s2gc, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (NT *)J->V);
+    CK(launch_chain(pdl, k_s2g<3, 8>, J->nb_s2g8, SGT_THREADS, J->smem_s2g8, s,
+                    (const float4 *)J->sorted, J->st, (const int4 *)J->chunks, (NT *)J->V));
+  CK(launch_chain(pdl, k_s2g_cell<D>, J->nb_s2gc, SGT_THREADS, 0, s, (const float4 *)J->sorted,
+                  J->st, (const int4 *)J->chunks, (NT *)J->V));
   if (ev) CK(cudaEventRecord(ev[2], s));
   CK(cudaGetLastError());
   return SGT_OK;
@@ -587,10 +662,11 @@ static sgt_status enqueue_gather_part(sgt_job *J, cudaStream_t s, cudaEvent_t *e
   sgt_ctx *ctx = J->ctx;
   typedef typename Vec<D>::T VT;
   typedef typename Node<D>::T NT;
-  CKS(enqueue_g2g<D>(J, s));
+  const bool pdl = ev == nullptr;
+  CKS(enqueue_g2g<D>(J, s, pdl));
   if (ev) CK(cudaEventRecord(ev[3], s));
-  k_g2s<D><<<J->nb_g2s, SGT_THREADS, 0, s>>>(J->sorted, J->st, J->chunks, (const NT *)J->Phi,
-                                             (VT *)J->Frep, J->part_z, J->n);
+  CK(launch_chain(pdl, k_g2s<D>, J->nb_g2s, SGT_THREADS, 0, s, (const float4 *)J->sorted, J->st,
+                  (const int4 *)J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n));
   CK(cudaGetLastError());
   return SGT_OK;
 }
@@ -823,7 +899,7 @@ static sgt_status tune_group_d(sgt_job *J) {
   // coordinates for every point P's columns index, forces for its rows
   const size_t np = (size_t)std::max(J->n, J->n_gather) * J->S;
   float *buf = nullptr;
-  CK(cudaMallocAsync(&buf, sizeof(float) * np * 2, s));
+  CK(sgti_alloc(ctx, (void **)&buf, sizeof(float) * np * 2, s));
   CK(cudaMemsetAsync(buf, 0, sizeof(float) * np * 2, s));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -1034,7 +1110,7 @@ static sgt_status job_create_impl(sgt_ctx *ctx, const sgt_params *params, int n,
   if (!mem_is_device) CKS(check_csr(ctx, n, hrp.data(), col, ncols));
   if (mem_is_device) {
     int *bad = nullptr;
-    CK(cudaMallocAsync(&bad, sizeof(int), s));
+    CK(sgti_alloc(ctx, (void **)&bad, sizeof(int), s));
     CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
     k_validate_csr<<<grid_blocks(ctx->nsm, 4), SGT_THREADS, 0, s>>>(n, ncols, rowptr, col, bad);
     int hb = 0;
@@ -1089,8 +1165,8 @@ static sgt_status job_create_impl(sgt_ctx *ctx, const sgt_params *params, int n,
       dcol = (int *)col;
       dval = (float *)val;
     } else {
-      if (cudaMallocAsync(&dcol, sizeof(int) * nnz, s) != cudaSuccess ||
-          cudaMallocAsync(&dval, sizeof(float) * nnz, s) != cudaSuccess)
+      if (sgti_alloc(ctx, (void **)&dcol, sizeof(int) * nnz, s) != cudaSuccess ||
+          sgti_alloc(ctx, (void **)&dval, sizeof(float) * nnz, s) != cudaSuccess)
         return bail(fail(ctx, SGT_ERR_NO_MEMORY, "staging P"));
       cudaMemcpyAsync(dcol, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, s);
       cudaMemcpyAsync(dval, val, sizeof(float) * nnz, cudaMemcpyHostToDevice, s);
@@ -1194,7 +1270,7 @@ sgt_status sgt_job_set_y(sgt_job *J, const float *y, int layout, int mem_is_devi
   const float *src = y;
   float *staging = nullptr;
   if (!mem_is_device) {
-    CK(cudaMallocAsync(&staging, bytes, s));
+    CK(sgti_alloc(ctx, (void **)&staging, bytes, s));
     CK(cudaMemcpyAsync(staging, y, bytes, cudaMemcpyHostToDevice, s));
     src = staging;
   }
@@ -1366,7 +1442,7 @@ sgt_status sgt_job_run(sgt_job *J, int iters) {
 // table of block counts per stage, and one view/prefix table per row-group
 // lane count for the SpMV.
 enum {
-  FS_BIN_COUNT, FS_BIN_SCAN, FS_BIN_SCATTER, FS_S2G, FS_S2G8, FS_S2G_CELL, FS_FFT_X,
+  FS_BIN_COUNT, FS_BIN_SCATTER, FS_S2G, FS_S2G8, FS_S2G_CELL, FS_FFT_X,
   FS_FFT_MID_FWD, FS_FFT_LAST, FS_FFT_MID_INV, FS_FFT_FINAL, FS_G2S, FS_UPDATE, FS_STAGES
 };
 struct BatchGroup {
@@ -1472,9 +1548,8 @@ static void stage_blocks(const sgt_job *J, int *b, int *nb_s2g2) {
   for (int k = 0; k < FS_STAGES; k++) b[k] = 0;
   const int work = std::max(1, (J->n + 2047) / 2048);
   const int s2g = std::min(J->nb_s2g, work);
-  b[FS_BIN_COUNT] = std::min(J->nb_pts, work);
-  b[FS_BIN_SCAN] = 1;
-  b[FS_BIN_SCATTER] = std::min(J->nb_pts, work);
+  b[FS_BIN_COUNT] = std::min(J->nb_bin, work);
+  b[FS_BIN_SCATTER] = std::min(J->nb_bin, work);
   b[FS_S2G] = s2g;
   if (J->d == 3) b[FS_S2G8] = std::min(J->nb_s2g8, 2 * work);
   b[FS_S2G_CELL] = std::min(J->nb_s2gc, 2 * work);
@@ -1585,7 +1660,7 @@ static sgt_status batch_fused_tables(sgt_batch *b) {
   sgt_ctx *ctx = b->ctx;
   FusedImage im;
   build_fused_image(b->jobs, im);
-  CK(cudaMallocAsync(&b->dmem, im.bytes(), ctx->stream));
+  CK(sgti_alloc(ctx, (void **)&b->dmem, im.bytes(), ctx->stream));
   CKS(bind_fused_image(ctx, im, b->dmem, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));  // the host image goes out of scope
   b->groups = im.groups;
@@ -1616,7 +1691,6 @@ static sgt_status enqueue_fused_group(sgt_ctx *ctx, BatchGroup &g) {
   }
   CK(cudaEventRecord(g.ev_spmv, sd));
   km_bin_count<D><<<FL(FS_BIN_COUNT), 0, c>>>(v, g.prefix[FS_BIN_COUNT], nj);
-  km_bin_scan<<<g.blocks[FS_BIN_SCAN], 1024, 0, c>>>(v, g.prefix[FS_BIN_SCAN], nj);
   km_bin_scatter<D><<<FL(FS_BIN_SCATTER), 0, c>>>(v, g.prefix[FS_BIN_SCATTER], nj);
   constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
   km_s2g<D, TT><<<FL(FS_S2G), g.smem_s2g, c>>>(v, g.prefix[FS_S2G], nj);
@@ -1721,7 +1795,7 @@ sgt_status sgt_batch_step(sgt_ctx *ctx, int njobs, sgt_job *const *jobs, int ite
     ctx->step_tables = nullptr;
     ctx->step_bytes = 0;
     const size_t want = std::max(im.bytes() * 2, (size_t)1 << 16);
-    CK(cudaMallocAsync(&ctx->step_tables, want, s));
+    CK(sgti_alloc(ctx, (void **)&ctx->step_tables, want, s));
     ctx->step_bytes = want;
   }
   CKS(bind_fused_image(ctx, im, ctx->step_tables, s));
@@ -1982,7 +2056,7 @@ sgt_status sgt_shard_set_y(sgt_shard *sh, const float *y, int layout, int mem_is
   const float *src = y;
   float *staging = nullptr;
   if (!mem_is_device) {
-    CK(cudaMallocAsync(&staging, bytes, s));
+    CK(sgti_alloc(ctx, (void **)&staging, bytes, s));
     CK(cudaMemcpyAsync(staging, y, bytes, cudaMemcpyHostToDevice, s));
     src = staging;
   }
@@ -2048,7 +2122,7 @@ sgt_status sgt_shard_get_y(sgt_shard *sh, float *y, int layout, int mem_is_devic
   const size_t bytes = sizeof(float) * (size_t)sh->n_all * J->d;
   float *dst = y, *staging = nullptr;
   if (!mem_is_device) {
-    CK(cudaMallocAsync(&staging, bytes, s));
+    CK(sgti_alloc(ctx, (void **)&staging, bytes, s));
     dst = staging;
   }
   // the mean over every point (the update phase leaves the own rows' one)
@@ -2131,7 +2205,7 @@ sgt_status sgt_job_get_y(sgt_job *J, float *y, int layout, int mem_is_device, in
   const size_t bytes = sizeof(float) * (size_t)J->n * J->d;
   float *dst = y, *staging = nullptr;
   if (!mem_is_device) {
-    CK(cudaMallocAsync(&staging, bytes, s));
+    CK(sgti_alloc(ctx, (void **)&staging, bytes, s));
     dst = staging;
   }
   const int nb = grid_blocks(ctx->nsm, 4);
@@ -2598,8 +2672,8 @@ static sgt_status job_rep_error(sgt_job *J, double *out) {
   typedef typename Vec<D>::T VT;
   const int n = J->n;
   double *num = nullptr, *z = nullptr;
-  CK(cudaMallocAsync(&num, sizeof(double) * (size_t)n * D, s));
-  CK(cudaMallocAsync(&z, sizeof(double) * (size_t)n, s));
+  CK(sgti_alloc(ctx, (void **)&num, sizeof(double) * (size_t)n * D, s));
+  CK(sgti_alloc(ctx, (void **)&z, sizeof(double) * (size_t)n, s));
   k_frep_exact<D><<<(n + SGT_THREADS - 1) / SGT_THREADS, SGT_THREADS, 0, s>>>((const VT *)J->Y, n,
                                                                               num, z);
   std::vector<double> hn((size_t)n * D), hz((size_t)n);
@@ -2669,12 +2743,12 @@ extern "C" sgt_status sgt_embed(sgt_ctx *ctx, int n, const int *rowptr, const in
     for (void *q : {(void *)drp, (void *)dc, (void *)dv, (void *)srp, (void *)sc, (void *)sv})
       if (q) cudaFreeAsync(q, s);
   };
-  cudaError_t ae = cudaMallocAsync(&drp, sizeof(int) * ((size_t)n + 1), s);
-  if (ae == cudaSuccess) ae = cudaMallocAsync(&dc, sizeof(int) * (size_t)std::max(nnz, 1L), s);
-  if (ae == cudaSuccess) ae = cudaMallocAsync(&dv, sizeof(float) * (size_t)std::max(nnz, 1L), s);
-  if (ae == cudaSuccess) ae = cudaMallocAsync(&srp, sizeof(int) * ((size_t)n + 1), s);
-  if (ae == cudaSuccess) ae = cudaMallocAsync(&sc, sizeof(int) * (size_t)std::max(2 * nnz, 1L), s);
-  if (ae == cudaSuccess) ae = cudaMallocAsync(&sv, sizeof(float) * (size_t)std::max(2 * nnz, 1L), s);
+  cudaError_t ae = sgti_alloc(ctx, (void **)&drp, sizeof(int) * ((size_t)n + 1), s);
+  if (ae == cudaSuccess) ae = sgti_alloc(ctx, (void **)&dc, sizeof(int) * (size_t)std::max(nnz, 1L), s);
+  if (ae == cudaSuccess) ae = sgti_alloc(ctx, (void **)&dv, sizeof(float) * (size_t)std::max(nnz, 1L), s);
+  if (ae == cudaSuccess) ae = sgti_alloc(ctx, (void **)&srp, sizeof(int) * ((size_t)n + 1), s);
+  if (ae == cudaSuccess) ae = sgti_alloc(ctx, (void **)&sc, sizeof(int) * (size_t)std::max(2 * nnz, 1L), s);
+  if (ae == cudaSuccess) ae = sgti_alloc(ctx, (void **)&sv, sizeof(float) * (size_t)std::max(2 * nnz, 1L), s);
   if (ae == cudaSuccess) ae = cudaMemcpyAsync(drp, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, s);
   if (ae == cudaSuccess) ae = cudaMemcpyAsync(dc, col, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s);
   if (ae == cudaSuccess) ae = cudaMemcpyAsync(dv, val, sizeof(float) * (size_t)nnz, cudaMemcpyHostToDevice, s);

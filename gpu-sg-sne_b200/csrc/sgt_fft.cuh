@@ -28,6 +28,9 @@
 #define SGT_FFT_COLS 8  // columns per CTA in column passes (one per warp)
 #define SGT_FFT_PAD 1   // float2 padding per staged column
 #define SGT_FFT_MAXM 1024  // longest FFT: twiddle tables hold M entries
+// d = 2 grids with M <= SGT_FFT_SMALL_M: the whole convolution runs in one CTA
+// in shared memory (conv2d_small_body), and the row passes return at once
+#define SGT_FFT_SMALL_M 64
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -218,6 +221,7 @@ __device__ void conv1d_body(const SgtState *st, const float2 *__restrict__ V, fl
 }
 
 __device__ __forceinline__ void k_conv1d_body(int vb_, int vg_, const SgtState *st, const float2 *__restrict__ V, float2 *__restrict__ Phi) {
+  sgt_pdl_wait();
   __shared__ float2 tw[SGT_FFT_MAXM];
   fft_twiddles(tw, st->M);
   __syncthreads();
@@ -277,7 +281,9 @@ __device__ void build_rows_body(int vb_, int vg_, const SgtState *st, const type
 
 template <int D>
 __device__ __forceinline__ void k_fft_build_x_body(int vb_, int vg_, const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
+  sgt_pdl_wait();
   __shared__ float2 tw[SGT_FFT_MAXM];
+  if (D == 2 && st->M <= SGT_FFT_SMALL_M) return;  // the column pass does it all
   fft_twiddles(tw, st->M);
   __syncthreads();
 #define CB(L) build_rows_body<D, L>(vb_, vg_, st, V, W, tw)
@@ -288,6 +294,95 @@ template <int D>
 __global__ void __launch_bounds__(SGT_THREADS)
 k_fft_build_x(const SgtState *st, const typename Node<D>::T *__restrict__ V, float2 *__restrict__ W) {
   k_fft_build_x_body<D>(blockIdx.x, gridDim.x, st, V, W);
+}
+
+// ---------------------------------------------------------------------------
+// d = 2, M <= SGT_FFT_SMALL_M: the three passes below in one CTA, with the
+// planes in shared memory (rows padded to M + 1 points so that the column
+// reads of the lanes fall in distinct banks).  The same transforms, products
+// and scaling in the same order as the multi-CTA passes, so the potentials
+// are the same; small grids (the h-driven grids of most runs) save two
+// passes through global memory and the launch latency between them.
+// Shared memory: twiddles (M), the kernel plane (M rows), the data planes
+// (2 x N rows, N <= M / 2).
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ void conv2d_small_body(const SgtState *st, const float4 *__restrict__ V,
+                                  float2 *__restrict__ Phi2, float2 *sm) {
+  constexpr int E = M / 32, LS = M + 1;
+  const int N = st->N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const float hsq = st->h_eff * st->h_eff;
+  float2 *tw = sm;
+  float2 *kp = sm + M;
+  float2 *dp = kp + M * LS;  // plane p, row y at dp + (p N + y) LS
+  fft_twiddles(tw, M);
+  __syncthreads();
+  // rows along x: the kernel plane (all M rows), the data planes (y < N)
+  for (int ln = warp; ln < M + 2 * N; ln += nw) {
+    float2 v[E];
+    float2 *row;
+    if (ln < M) {
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = make_float2(kern_val(hsq, M, lane + 32 * e, ln, 0), 0.f);
+      row = kp + ln * LS;
+    } else {
+      const int r = ln - M, p = r / N, y = r % N;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int x = lane + 32 * e;
+        v[e] = x < N ? node_plane<2>(V[x + (long)N * y], p) : make_float2(0.f, 0.f);
+      }
+      row = dp + (p * N + y) * LS;
+    }
+    wfft_dif<M>(v, tw);
+#pragma unroll
+    for (int e = 0; e < E; e++) row[lane + 32 * e] = v[e];
+  }
+  __syncthreads();
+  // columns along y: the kernel spectrum (real part), then per data plane
+  // forward, product, inverse; rows y >= N of the data are zero and dropped
+  for (int c = warp; c < M; c += nw) {
+    float2 v[E];
+    float kr[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = kp[(lane + 32 * e) * LS + c];
+    wfft_dif<M>(v, tw);
+#pragma unroll
+    for (int e = 0; e < E; e++) kr[e] = v[e].x;
+    for (int p = 0; p < 2; p++) {
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int y = lane + 32 * e;
+        v[e] = y < N ? dp[(p * N + y) * LS + c] : make_float2(0.f, 0.f);
+      }
+      wfft_dif<M>(v, tw);
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = make_float2(v[e].x * kr[e], v[e].y * kr[e]);
+      wfft_dit_inv<M>(v, tw);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int y = lane + 32 * e;
+        if (y < N) dp[(p * N + y) * LS + c] = v[e];
+      }
+    }
+  }
+  __syncthreads();
+  // rows inverse along x, scaled by 1/M^2, into the potential grid
+  float inv = 1.0f / (float)M;
+  inv = inv / (float)M;
+  for (int ln = warp; ln < 2 * N; ln += nw) {
+    const int p = ln % 2, y = ln / 2;
+    float2 v[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = dp[(p * N + y) * LS + lane + 32 * e];
+    wfft_dit_inv<M>(v, tw);
+    const long g0 = (long)N * y;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int x = lane + 32 * e;
+      if (x < N) Phi2[2 * (g0 + x) + p] = make_float2(v[e].x * inv, v[e].y * inv);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -403,8 +498,20 @@ __device__ void cols_body(int vb_, int vg_, const SgtState *st, float2 *__restri
 }
 
 template <int D, int MODE>
-__device__ __forceinline__ void k_fft_cols_body(int vb_, int vg_, const SgtState *st, float2 *__restrict__ W) {
+__device__ __forceinline__ void k_fft_cols_body(int vb_, int vg_, const SgtState *st, float2 *__restrict__ W,
+                                                const typename Node<D>::T *__restrict__ V,
+                                                typename Node<D>::T *__restrict__ Phi) {
+  sgt_pdl_wait();
   extern __shared__ float2 sm[];
+  if constexpr (D == 2 && MODE == MODE_LAST) {
+    if (st->M <= SGT_FFT_SMALL_M) {  // block-uniform
+      if (vb_ == 0) {
+        if (st->M == 32) conv2d_small_body<32>(st, V, reinterpret_cast<float2 *>(Phi), sm);
+        else conv2d_small_body<64>(st, V, reinterpret_cast<float2 *>(Phi), sm);
+      }
+      return;
+    }
+  }
   float2 *tw = sm;
   float2 *stg = sm + SGT_FFT_MAXM;
   float *kre = reinterpret_cast<float *>(stg + SGT_FFT_COLS * (st->M + SGT_FFT_PAD));
@@ -416,8 +523,9 @@ __device__ __forceinline__ void k_fft_cols_body(int vb_, int vg_, const SgtState
 }
 template <int D, int MODE>
 __global__ void __launch_bounds__(SGT_THREADS)
-k_fft_cols(const SgtState *st, float2 *__restrict__ W) {
-  k_fft_cols_body<D, MODE>(blockIdx.x, gridDim.x, st, W);
+k_fft_cols(const SgtState *st, float2 *__restrict__ W, const typename Node<D>::T *__restrict__ V,
+           typename Node<D>::T *__restrict__ Phi) {
+  k_fft_cols_body<D, MODE>(blockIdx.x, gridDim.x, st, W, V, Phi);
 }
 
 // ---------------------------------------------------------------------------
@@ -455,7 +563,9 @@ __device__ void final_rows_body(int vb_, int vg_, const SgtState *st, const floa
 
 template <int D>
 __device__ __forceinline__ void k_fft_final_x_body(int vb_, int vg_, const SgtState *st, const float2 *__restrict__ W, typename Node<D>::T *__restrict__ Phi) {
+  sgt_pdl_wait();
   __shared__ float2 tw[SGT_FFT_MAXM];
+  if (D == 2 && st->M <= SGT_FFT_SMALL_M) return;  // the column pass did it all
   fft_twiddles(tw, st->M);
   __syncthreads();
 #define CF(L) final_rows_body<D, L>(vb_, vg_, st, W, reinterpret_cast<float2 *>(Phi), tw)
@@ -468,8 +578,15 @@ k_fft_final_x(const SgtState *st, const float2 *__restrict__ W, typename Node<D>
   k_fft_final_x_body<D>(blockIdx.x, gridDim.x, st, W, Phi);
 }
 
-// shared memory of a column pass for FFT length Mmax
-__host__ __device__ inline size_t fft_cols_smem(int Mmax) {
-  return sizeof(float2) * (SGT_FFT_MAXM + (size_t)SGT_FFT_COLS * (Mmax + SGT_FFT_PAD)) +
-         sizeof(float) * (size_t)SGT_FFT_COLS * Mmax;
+// shared memory of a column pass for FFT length Mmax; in d = 2 also enough
+// for the one-CTA convolution of the small lengths that Mmax admits
+__host__ __device__ inline size_t fft_cols_smem(int Mmax, int d = 3) {
+  size_t b = sizeof(float2) * (SGT_FFT_MAXM + (size_t)SGT_FFT_COLS * (Mmax + SGT_FFT_PAD)) +
+             sizeof(float) * (size_t)SGT_FFT_COLS * Mmax;
+  if (d == 2) {
+    const size_t m = Mmax < SGT_FFT_SMALL_M ? (size_t)Mmax : (size_t)SGT_FFT_SMALL_M;
+    const size_t small = sizeof(float2) * (m + m * (m + 1) + m * (m + 1));  // twiddles, kernel, 2 x m/2 data rows
+    if (small > b) b = small;
+  }
+  return b;
 }

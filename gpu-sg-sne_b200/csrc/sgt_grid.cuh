@@ -232,13 +232,96 @@ k_init_stats(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
 
 
 // ---------------------------------------------------------------------------
+// bin scan (run by the last block of bin_count): tile offsets and the chunk
+// work list
+// ---------------------------------------------------------------------------
+// exclusive scan over the threads of a block (blockDim a multiple of 32)
+__device__ __forceinline__ int block_exclusive_scan(int v, int *total) {
+  __shared__ int wsum[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    wsum[lane] = s;
+  }
+  __syncthreads();
+  const int excl = x - v + (w > 0 ? wsum[w - 1] : 0);
+  *total = wsum[nw - 1];
+  __syncthreads();
+  return excl;
+}
+
+// Thread t owns the tiles [t per, t per + per); the counts (written by other
+// blocks' atomics) are read from L2.
+__device__ __forceinline__ void bin_scan_block(SgtState *st, const SgtJobParams &jp,
+                                               int *__restrict__ tile_count,
+                                               int *__restrict__ cursor,
+                                               int4 *__restrict__ chunks, int nblk) {
+  const int ntiles = st->ntiles;
+  // chunk length: about two chunks per persistent S2G CTA, at least 1024
+  // points (256 in 3-D, where a point costs 64 nodes and small jobs need more
+  // chunks than they have 1024-point runs)
+  int chunk = (jp.n + 2 * nblk - 1) / (2 * nblk);
+  chunk = ((chunk + 255) / 256) * 256;
+  const int cmin = jp.chunk_min > 0 ? jp.chunk_min : (jp.d == 3 ? 256 : 1024);
+  if (chunk < cmin) chunk = cmin;
+  const int per = (ntiles + blockDim.x - 1) / blockDim.x;
+  const int t0 = threadIdx.x * per, t1 = min(t0 + per, ntiles);
+  int mysum = 0, mych = 0;
+  for (int t = t0; t < t1; t++) {
+    const int c = __ldcg(&tile_count[t]);
+    mysum += c;
+    mych += (c + chunk - 1) / chunk;
+  }
+  int tot_pts, tot_ch;
+  int base = block_exclusive_scan(mysum, &tot_pts);
+  int cbase = block_exclusive_scan(mych, &tot_ch);
+  for (int t = t0; t < t1; t++) {
+    const int cnt = __ldcg(&tile_count[t]);
+    const int cpt = (cnt + chunk - 1) / chunk;
+    cursor[t] = base;
+    for (int c = 0; c < cpt; c++) {
+      const int idx = cbase + c;
+      if (idx < jp.chunk_cap) {
+        const int len = min(chunk, cnt - c * chunk);
+        chunks[idx] = make_int4(t, base + c * chunk, len, 0);
+      }
+    }
+    base += cnt;
+    cbase += cpt;
+    tile_count[t] = 0;  // ready for the next iteration
+  }
+  if (threadIdx.x == 0) {
+    st->chunk = chunk;
+    if (tot_ch > jp.chunk_cap) {
+      st->error |= SGT_EFLAG_CHUNK_OVERFLOW;
+      tot_ch = jp.chunk_cap;
+    }
+    st->nchunks = tot_ch;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // bin_count: centre (Y = Ynext - mean), zero the grid V, count points per tile
 // ---------------------------------------------------------------------------
 template <int D>
 __device__ __forceinline__ void k_bin_count_body(int vb_, int vg_, const typename Vec<D>::T *__restrict__ Ynext,
             typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
             int *__restrict__ tile_count, typename Node<D>::T *__restrict__ V,
-            int write_centred) {
+            int write_centred, const SgtJobParams &jp, int *__restrict__ cursor,
+            int4 *__restrict__ chunks, int nblk) {
   __shared__ int hist[SGT_HIST_MAX];
   const int ntiles = st->ntiles, T = st->T, td = st->tiles_dim, N = st->N;
   const float maxy = st->maxy, scale = st->scale;
@@ -295,97 +378,32 @@ __device__ __forceinline__ void k_bin_count_body(int vb_, int vg_, const typenam
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
     if (hist[t]) atomicAdd(&tile_count[t], hist[t]);
+  // the last block to finish turns the tile counts into tile offsets and
+  // the chunk list (no separate launch between the count and the sort)
+  // (the barrier orders the block's count atomics before thread 0's
+  // device-scope fence, which is cumulative over them)
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&st->done_bin, 1u) == (unsigned)vg_ - 1u;
+    __threadfence();
+  }
+  __syncthreads();
+  if (last) {
+    bin_scan_block(st, jp, tile_count, cursor, chunks, nblk);
+    if (threadIdx.x == 0) st->done_bin = 0;
+  }
 }
 template <int D>
 __global__ void __launch_bounds__(SGT_THREADS)
 k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
             typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
             int *__restrict__ tile_count, typename Node<D>::T *__restrict__ V,
-            int write_centred) {
-  k_bin_count_body<D>(blockIdx.x, gridDim.x, Ynext, Y, n, st, tile_count, V, write_centred);
-}
-
-// ---------------------------------------------------------------------------
-// bin_scan (one CTA of 1024 threads): tile offsets and the chunk work list
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int block_exclusive_scan_1024(int v, int *total) {
-  __shared__ int wsum[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsum[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    int s = wsum[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
-    }
-    wsum[lane] = s;
-  }
-  __syncthreads();
-  const int excl = x - v + (w > 0 ? wsum[w - 1] : 0);
-  *total = wsum[31];
-  __syncthreads();
-  return excl;
-}
-
-__device__ __forceinline__ void k_bin_scan_body(int vb_, int vg_, SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
-           int *__restrict__ cursor, int4 *__restrict__ chunks, int nblk) {
-  const int ntiles = st->ntiles;
-  // chunk length: about two chunks per persistent CTA, at least 1024 points
-  // (256 in 3-D, where a point costs 64 nodes and small jobs need more
-  // chunks than they have 1024-point runs)
-  int chunk = (jp.n + 2 * nblk - 1) / (2 * nblk);
-  chunk = ((chunk + 255) / 256) * 256;
-  const int cmin = jp.chunk_min > 0 ? jp.chunk_min : (jp.d == 3 ? 256 : 1024);
-  if (chunk < cmin) chunk = cmin;
-  const int per = (ntiles + 1023) / 1024;  // <= 4
-  int cnt[4], cpt[4];
-  int mysum = 0, mych = 0;
-  for (int j = 0; j < per; j++) {
-    const int t = threadIdx.x * per + j;
-    cnt[j] = t < ntiles ? tile_count[t] : 0;
-    cpt[j] = (cnt[j] + chunk - 1) / chunk;
-    mysum += cnt[j];
-    mych += cpt[j];
-  }
-  int tot_pts, tot_ch;
-  int base = block_exclusive_scan_1024(mysum, &tot_pts);
-  int cbase = block_exclusive_scan_1024(mych, &tot_ch);
-  for (int j = 0; j < per; j++) {
-    const int t = threadIdx.x * per + j;
-    if (t >= ntiles) break;
-    cursor[t] = base;
-    for (int c = 0; c < cpt[j]; c++) {
-      const int idx = cbase + c;
-      if (idx < jp.chunk_cap) {
-        const int len = min(chunk, cnt[j] - c * chunk);
-        chunks[idx] = make_int4(t, base + c * chunk, len, 0);
-      }
-    }
-    base += cnt[j];
-    cbase += cpt[j];
-    tile_count[t] = 0;  // ready for the next iteration
-  }
-  if (threadIdx.x == 0) {
-    st->chunk = chunk;
-    if (tot_ch > jp.chunk_cap) {
-      st->error |= SGT_EFLAG_CHUNK_OVERFLOW;
-      tot_ch = jp.chunk_cap;
-    }
-    st->nchunks = tot_ch;
-  }
-}
-__global__ void __launch_bounds__(1024)
-k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
-           int *__restrict__ cursor, int4 *__restrict__ chunks, int nblk) {
-  k_bin_scan_body(blockIdx.x, gridDim.x, st, jp, tile_count, cursor, chunks, nblk);
+            int write_centred, SgtJobParams jp, int *__restrict__ cursor,
+            int4 *__restrict__ chunks, int nblk) {
+  k_bin_count_body<D>(blockIdx.x, gridDim.x, Ynext, Y, n, st, tile_count, V, write_centred,
+                      jp, cursor, chunks, nblk);
 }
 
 // ---------------------------------------------------------------------------
@@ -398,6 +416,7 @@ k_bin_scan(SgtState *st, SgtJobParams jp, int *__restrict__ tile_count,
 template <int D>
 __device__ __forceinline__ void k_bin_scatter_body(int vb_, int vg_, const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
               int *__restrict__ cursor, float4 *__restrict__ sorted) {
+  sgt_pdl_wait();
   __shared__ int lc[SGT_HIST_MAX];
   const int ntiles = st->ntiles, T = st->T, td = st->tiles_dim;
   const float maxy = st->maxy, scale = st->scale;
@@ -504,6 +523,7 @@ __device__ __forceinline__ void sgt_point_stencil(const float4 &rec,
 template <int D, int TT>
 __device__ __forceinline__ void k_s2g_body(int vb_, int vg_, const float4 *__restrict__ sorted, SgtState *st,
       const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
+  sgt_pdl_wait();
   extern __shared__ float acc[];  // [D+1][R^D]
   const int T = st->T, td = st->tiles_dim, N = st->N, nch = st->nchunks;
   if (T != TT) return;
@@ -669,6 +689,7 @@ k_s2g(const float4 *__restrict__ sorted, SgtState *st,
 template <int D>
 __device__ __forceinline__ void k_s2g_cell_body(int vb_, int vg_, const float4 *__restrict__ sorted, SgtState *st,
            const int4 *__restrict__ chunks, typename Node<D>::T *__restrict__ V) {
+  sgt_pdl_wait();
   if (st->T != 1) return;  // tile mode: k_s2g does the work
   constexpr int NN = D == 1 ? 4 : 16;  // stencil nodes per pass
   constexpr int C = D + 1;             // charge channels
@@ -809,6 +830,7 @@ __device__ __forceinline__ void k_g2s_body(int vb_, int vg_, const float4 *__res
       const int4 *__restrict__ chunks,
       const typename Node<D>::T *__restrict__ Phi,
       typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n) {
+  sgt_pdl_wait();
   __shared__ double wz[SGT_THREADS / 32];
   __shared__ bool last;
   const int N = st->N, nch = st->nchunks;

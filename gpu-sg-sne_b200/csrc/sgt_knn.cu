@@ -599,7 +599,7 @@ static sgt_status knn_tc(sgt_ctx *ctx, int n, int dim, const float *X, int k, in
   const size_t o_nrm = 2 * img_bytes, o_max = o_nrm + sizeof(float) * (size_t)nblk * KNN_TC_M;
   const size_t o_cnt = o_max + 16, o_redo = o_cnt + 16;
   const size_t total = o_redo + sizeof(int) * (size_t)n;
-  cudaError_t e = cudaMallocAsync(&buf, total, s);
+  cudaError_t e = sgti_alloc(ctx, (void **)&buf, total, s);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();  // not sticky: clear it for the caller's next check
     return sgti_fail(ctx, SGT_ERR_NO_MEMORY, "sgt_knn: tensor-core operand images");

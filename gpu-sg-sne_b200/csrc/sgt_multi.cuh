@@ -56,13 +56,7 @@ km_bin_count(const SgtJobView *__restrict__ views, const int *__restrict__ prefi
   SGT_MULTI_JOB
   typedef typename Vec<D>::T VT;
   k_bin_count_body<D>(vb, vg, (const VT *)v.Ynext_c, (VT *)v.Y, v.n, v.st, v.tile_count,
-                      (typename Node<D>::T *)v.V, 1);
-}
-
-__global__ void __launch_bounds__(1024)
-km_bin_scan(const SgtJobView *__restrict__ views, const int *__restrict__ prefix, int njobs) {
-  SGT_MULTI_JOB
-  k_bin_scan_body(vb, vg, v.st, v.jp, v.tile_count, v.cursor, v.chunks, v.nb_s2g);
+                      (typename Node<D>::T *)v.V, 1, v.jp, v.cursor, v.chunks, v.nb_s2g);
 }
 
 template <int D>
@@ -103,7 +97,8 @@ template <int D, int MODE>
 __global__ void __launch_bounds__(SGT_THREADS)
 km_fft_cols(const SgtJobView *__restrict__ views, const int *__restrict__ prefix, int njobs) {
   SGT_MULTI_JOB
-  k_fft_cols_body<D, MODE>(vb, vg, v.st, v.W);
+  k_fft_cols_body<D, MODE>(vb, vg, v.st, v.W, (const typename Node<D>::T *)v.V,
+                           (typename Node<D>::T *)v.Phi);
 }
 
 template <int D>

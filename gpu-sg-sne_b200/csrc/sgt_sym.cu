@@ -122,15 +122,15 @@ extern "C" sgt_status sgt_symmetrize_device(sgt_ctx *ctx, int n, long nnz, const
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, head, pos, (int)m, s);
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_rows, cnt, out_rowptr, n + 1, s);
   const size_t tmp_bytes = std::max(tmp_sort, std::max(tmp_scan, tmp_rows));
-  ok(cudaMallocAsync(&k0, sizeof(unsigned long long) * m, s));
-  ok(cudaMallocAsync(&k1, sizeof(unsigned long long) * m, s));
-  ok(cudaMallocAsync(&v0, sizeof(float) * m, s));
-  ok(cudaMallocAsync(&v1, sizeof(float) * m, s));
-  ok(cudaMallocAsync(&head, sizeof(int) * m, s));
-  ok(cudaMallocAsync(&pos, sizeof(int) * m, s));
-  ok(cudaMallocAsync(&cnt, sizeof(int) * ((size_t)n + 1), s));
-  ok(cudaMallocAsync(&bad, sizeof(int), s));
-  ok(cudaMallocAsync(&tmp, tmp_bytes, s));
+  ok(sgti_alloc(ctx, (void **)&k0, sizeof(unsigned long long) * m, s));
+  ok(sgti_alloc(ctx, (void **)&k1, sizeof(unsigned long long) * m, s));
+  ok(sgti_alloc(ctx, (void **)&v0, sizeof(float) * m, s));
+  ok(sgti_alloc(ctx, (void **)&v1, sizeof(float) * m, s));
+  ok(sgti_alloc(ctx, (void **)&head, sizeof(int) * m, s));
+  ok(sgti_alloc(ctx, (void **)&pos, sizeof(int) * m, s));
+  ok(sgti_alloc(ctx, (void **)&cnt, sizeof(int) * ((size_t)n + 1), s));
+  ok(sgti_alloc(ctx, (void **)&bad, sizeof(int), s));
+  ok(sgti_alloc(ctx, (void **)&tmp, tmp_bytes, s));
   int hbad = 0, total = 0;
   if (e == cudaSuccess) {
     const int nb = (int)std::min<long>((nnz + SYM_THREADS - 1) / SYM_THREADS, 148L * 16);
