@@ -89,7 +89,14 @@ struct SgtJobParams {
   int tile_cap;       // max tiles held by the tile arrays
   int chunk_cap;      // max chunks held by the chunk array
   int chunk_min;      // fewest points per S2G chunk (0: 1024, 256 in 3-D)
+  int direct_max;     // largest N of a direct-mode grid (0: no direct mode)
 };
+
+// Direct mode (d <= 2): S2G and G2S work on the points in their own order
+// with the whole grid in shared memory, without the tile sort, on grids that
+// are not dense enough for cell mode.  2-D grids up to this many points per
+// axis (64^2 float4 nodes = 64 KB); 1-D grids always.
+#define SGT_DIRECT_N2 64
 
 template <int D> struct Vec;
 template <> struct Vec<1> { typedef float T; };

@@ -98,6 +98,7 @@ struct sgt_job {
       nb_upd = 0, nb_part = 0;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // the two branches of an iteration
   size_t smem_s2g = 0, smem_s2g8 = 0, smem_fft1 = 0, smem_fft2 = 0;
+  size_t smem_s2gd = 0, smem_g2sd = 0;  // direct-mode S2G and G2S (0: the job never takes it)
   int nb_s2g8 = 0;  // 3-D tiles of 8 cells
   cudaGraphExec_t gexec = nullptr;        // one iteration
   cudaGraphExec_t gexec_multi = nullptr;  // SGT_GRAPH_ITERS chained iterations
@@ -411,6 +412,21 @@ static sgt_status job_shapes(sgt_job *J) {
   }
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s2g_cell<D>, SGT_THREADS, 0));
   J->nb_s2gc = grid_blocks(nsm, occ);
+  // direct mode (d <= 2, jobs that can take it): the S2G's grid copy (m
+  // planes of N^d floats) and the G2S's potential grid (N^d nodes)
+  if constexpr (D <= 2) {
+    const size_t dn = (size_t)J->jp.direct_max;
+    const size_t dnodes = D == 1 ? dn : dn * dn;
+    J->smem_s2gd = sizeof(float) * (D + 1) * dnodes;
+    J->smem_g2sd = sizeof(typename Node<D>::T) * dnodes;
+    // the attributes allow the largest job of this dimension (jobs of other
+    // sizes set them too, and every job's launches must stay allowed)
+    const size_t dmax = D == 1 ? 512 : (size_t)SGT_DIRECT_N2 * SGT_DIRECT_N2;
+    CK(cudaFuncSetAttribute(k_s2g_direct<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(sizeof(float) * (D + 1) * dmax)));
+    CK(cudaFuncSetAttribute(k_g2s_direct<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(sizeof(typename Node<D>::T) * dmax)));
+  }
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2s<D>, SGT_THREADS, 0));
   J->nb_g2s = grid_blocks(nsm, occ);
   const int M = J->mmax;
@@ -419,10 +435,11 @@ static sgt_status job_shapes(sgt_job *J) {
   if constexpr (D == 1) {
     J->nb_fft = 1;
   } else {
-    CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+    const int fmax = (int)fft_cols_smem(SGT_FFT_MAXM, D);  // the largest job's
+    CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, fmax));
     if constexpr (D == 3) {
-      CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_MID_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
-      CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_MID_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)J->smem_fft2));
+      CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_MID_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, fmax));
+      CK(cudaFuncSetAttribute(k_fft_cols<D, MODE_MID_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, fmax));
     }
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fft_cols<D, MODE_LAST>, SGT_THREADS, J->smem_fft2));
     J->nb_fft = grid_blocks(nsm, occ);
@@ -509,6 +526,15 @@ static sgt_status job_alloc(sgt_job *J) {
   CKS(jalloc(J, &J->chunks, (size_t)J->jp.chunk_cap));
   J->jp.mmax = M;
   J->jp.tile_cap = SGT_HIST_MAX;
+  // direct mode for the grids up to direct_max that are too sparse for cell
+  // mode; a job with enough points that all of them are dense never takes it
+  // (and its kernels keep the small shared-memory footprint the concurrent
+  // SpMV wants: the direct mode's grid copies shrink the SMs' L1)
+  J->jp.direct_max = D == 1 ? J->nmax : (D == 2 ? std::min(SGT_DIRECT_N2, J->nmax) : 0);
+  if (J->jp.direct_max > 0) {
+    const long c = J->jp.direct_max - 3, dense = 64L * (D == 1 ? c : c * c);
+    if ((long)J->n >= dense && (D == 1 ? c : c * c) <= SGT_HIST_MAX) J->jp.direct_max = 0;
+  }
   CKS(jalloc(J, &J->st, 1));
   J->st_host = new SgtState();
   CK(cudaEventCreateWithFlags(&J->ev_fork, cudaEventDisableTiming));
@@ -629,7 +655,7 @@ static sgt_status enqueue_bin_count(sgt_job *J, cudaStream_t s) {
   return SGT_OK;
 }
 
-// Tile offsets, sort and S2G: the charge grid of this job's points.
+// Sort and S2G (or the direct S2G): the charge grid of this job's points.
 // ev (optional): events recorded after the binning and S2G stages.
 template <int D>
 static sgt_status enqueue_scatter_part(sgt_job *J, cudaStream_t s, cudaEvent_t *ev = nullptr) {
@@ -638,9 +664,15 @@ static sgt_status enqueue_scatter_part(sgt_job *J, cudaStream_t s, cudaEvent_t *
   typedef typename Node<D>::T NT;
   const int n = J->n;
   const bool pdl = ev == nullptr;
+  // the S2G stage starts with the sort (tile modes) or is the whole direct
+  // S2G (direct mode), both in k_bin_scatter
+  if (ev) CK(cudaEventRecord(ev[1], s));
   CK(launch_chain(pdl, k_bin_scatter<D>, J->nb_bin, SGT_THREADS, 0, s, (const VT *)J->Y, n, J->st,
                   J->cursor, J->sorted));
-  if (ev) CK(cudaEventRecord(ev[1], s));
+  if constexpr (D <= 2)
+    if (J->jp.direct_max > 0)
+      CK(launch_chain(pdl, k_s2g_direct<D>, J->nb_bin, SGT_THREADS, J->smem_s2gd, s,
+                      (const VT *)J->Y, n, J->st, (NT *)J->V));
   // tile mode and cell mode: the kernel of the other mode returns at once
   constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
   CK(launch_chain(pdl, k_s2g<D, TT>, J->nb_s2g, SGT_THREADS, J->smem_s2g, s,
@@ -667,6 +699,10 @@ static sgt_status enqueue_gather_part(sgt_job *J, cudaStream_t s, cudaEvent_t *e
   if (ev) CK(cudaEventRecord(ev[3], s));
   CK(launch_chain(pdl, k_g2s<D>, J->nb_g2s, SGT_THREADS, 0, s, (const float4 *)J->sorted, J->st,
                   (const int4 *)J->chunks, (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n));
+  if constexpr (D <= 2)
+    if (J->jp.direct_max > 0)
+      CK(launch_chain(pdl, k_g2s_direct<D>, J->nb_g2s, SGT_THREADS, J->smem_g2sd, s, J->st,
+                      (const NT *)J->Phi, (VT *)J->Frep, J->part_z, J->n, (const VT *)J->Y));
   CK(cudaGetLastError());
   return SGT_OK;
 }
@@ -1450,7 +1486,7 @@ struct BatchGroup {
   const SgtJobView *views = nullptr;
   const int *prefix[FS_STAGES] = {};
   int blocks[FS_STAGES] = {};
-  size_t smem_s2g = 0, smem_s2g8 = 0, smem_fft = 0;
+  size_t smem_s2g = 0, smem_s2g8 = 0, smem_fft = 0, smem_s2gd = 0, smem_g2sd = 0;
   // SpMV: one launch per lane count G present
   struct Spmv {
     int G = 16, njobs = 0, blocks = 0;
@@ -1597,6 +1633,8 @@ static void build_fused_image(const std::vector<sgt_job *> &jobs, FusedImage &im
       g.smem_s2g = std::max(g.smem_s2g, J->smem_s2g);
       g.smem_s2g8 = std::max(g.smem_s2g8, J->smem_s2g8);
       g.smem_fft = std::max(g.smem_fft, J->smem_fft2);
+      g.smem_s2gd = std::max(g.smem_s2gd, J->smem_s2gd);
+      g.smem_g2sd = std::max(g.smem_g2sd, J->smem_g2sd);
     }
     for (int k = 0; k < FS_STAGES; k++) {
       o.prefix[k] = im.ints.size();
@@ -1692,6 +1730,9 @@ static sgt_status enqueue_fused_group(sgt_ctx *ctx, BatchGroup &g) {
   CK(cudaEventRecord(g.ev_spmv, sd));
   km_bin_count<D><<<FL(FS_BIN_COUNT), 0, c>>>(v, g.prefix[FS_BIN_COUNT], nj);
   km_bin_scatter<D><<<FL(FS_BIN_SCATTER), 0, c>>>(v, g.prefix[FS_BIN_SCATTER], nj);
+  if constexpr (D <= 2)
+    if (g.smem_s2gd > 0)  // some job of the group can take the direct mode
+      km_s2g_direct<D><<<FL(FS_BIN_SCATTER), g.smem_s2gd, c>>>(v, g.prefix[FS_BIN_SCATTER], nj);
   constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
   km_s2g<D, TT><<<FL(FS_S2G), g.smem_s2g, c>>>(v, g.prefix[FS_S2G], nj);
   if constexpr (D == 3) km_s2g<3, 8><<<FL(FS_S2G8), g.smem_s2g8, c>>>(v, g.prefix[FS_S2G8], nj);
@@ -1708,6 +1749,9 @@ static sgt_status enqueue_fused_group(sgt_ctx *ctx, BatchGroup &g) {
     km_fft_final_x<D><<<FL(FS_FFT_FINAL), 0, c>>>(v, g.prefix[FS_FFT_FINAL], nj);
   }
   km_g2s<D><<<FL(FS_G2S), 0, c>>>(v, g.prefix[FS_G2S], nj);
+  if constexpr (D <= 2)
+    if (g.smem_g2sd > 0)
+      km_g2s_direct<D><<<FL(FS_G2S), g.smem_g2sd, c>>>(v, g.prefix[FS_G2S], nj);
   CK(cudaStreamWaitEvent(c, g.ev_spmv, 0));
   km_row_update<D><<<FL(FS_UPDATE), 0, c>>>(v, g.prefix[FS_UPDATE], nj);
   CK(cudaGetLastError());
@@ -1758,6 +1802,13 @@ static sgt_status batch_fused_graph(sgt_batch *b, int R, cudaGraphExec_t *exec) 
 template <int D>
 static sgt_status fused_attributes(sgt_ctx *ctx, const BatchGroup &g) {
   constexpr int TT = D == 1 ? 512 : (D == 2 ? 32 : 16);
+  if constexpr (D <= 2) {  // the largest any group of this dimension asks for
+    const size_t dmax = D == 1 ? 512 : (size_t)SGT_DIRECT_N2 * SGT_DIRECT_N2;
+    CK(cudaFuncSetAttribute(km_s2g_direct<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(sizeof(float) * (D + 1) * dmax)));
+    CK(cudaFuncSetAttribute(km_g2s_direct<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(sizeof(typename Node<D>::T) * dmax)));
+  }
   CK(cudaFuncSetAttribute(km_s2g<D, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_s2g));
   if constexpr (D == 3)
     CK(cudaFuncSetAttribute(km_s2g<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_s2g8));
@@ -2978,6 +3029,7 @@ extern "C" sgt_status sgt_repulsive_noalloc(sgt_ctx *ctx, int n, int d, float h,
   J.nmax = d == 1 ? 512 : SGT_NA_MAX_GRID_2D;
   J.jp.mmax = J.mmax;
   J.jp.tile_cap = SGT_HIST_MAX;
+  J.jp.direct_max = d == 1 ? J.nmax : std::min(SGT_DIRECT_N2, J.nmax);
   J.jp.chunk_cap = SGT_NA_CHUNKS;
   J.Y = (float *)(base + NA_Y);
   J.Ynext = (float *)(base + NA_YNEXT);

@@ -130,6 +130,14 @@ __device__ void sgt_finalize_grid(SgtState *st, const SgtJobParams &jp,
   // enough points each that one block reduction per chunk of a cell is
   // cheaper than shared-memory atomics that all land on a few nodes
   const bool cell_mode = ncell <= SGT_HIST_MAX && (long)jp.n >= 64L * ncell;
+  // direct mode (no sort, the grid in shared memory) for the other grids that
+  // fit: few points per node, so its shared-memory atomics rarely collide
+  if (!cell_mode && N <= jp.direct_max) {
+    st->T = 0;
+    st->tiles_dim = 0;
+    st->ntiles = 0;
+    return;
+  }
   // 3-D tiles of 8 cells while the tile count fits the tile arrays: a
   // (8+3)^3 x 4-channel shared accumulator is 21 KB (a 16-cell tile: 110 KB),
   // so each chunk zeroes and flushes 5x fewer nodes and more CTAs fit an SM
@@ -338,6 +346,30 @@ __device__ __forceinline__ void k_bin_count_body(int vb_, int vg_, const typenam
   for (long g = vb_ * (long)blockDim.x + threadIdx.x; g < nodes;
        g += (long)vg_ * blockDim.x)
     V[g] = z;
+  if (T == 0) {  // direct mode: centre only; k_bin_scatter does the S2G
+    if (write_centred) {
+      constexpr int U = SGT_PTS_U;
+      const long stride = (long)vg_ * blockDim.x * U;
+      for (long i0 = ((long)vb_ * blockDim.x + (threadIdx.x & ~31)) * U; i0 < n; i0 += stride) {
+        typename Vec<D>::T yv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const long i = i0 + 32 * u + (threadIdx.x & 31);
+          if (i < n) yv[u] = Ynext[i];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const long i = i0 + 32 * u + (threadIdx.x & 31);
+          if (i < n) {
+#pragma unroll
+            for (int k = 0; k < D; k++) setcomp<D>(yv[u], k, __fsub_rn(comp<D>(yv[u], k), mean[k]));
+            Y[i] = yv[u];
+          }
+        }
+      }
+    }
+    return;
+  }
   __syncthreads();
   // warp-uniform trip count: lanes with the same tile are merged with
   // match_any and add their count in one shared-memory atomic (points of an
@@ -407,6 +439,143 @@ k_bin_count(const typename Vec<D>::T *__restrict__ Ynext,
 }
 
 // ---------------------------------------------------------------------------
+// Direct-mode S2G (T = 0; d <= 2, grids of at most SGT_DIRECT_N2 points per
+// axis in 2-D that hold fewer than 64 points per cell): no sort.  A block takes a contiguous range of the points in
+// their own order, accumulates their weighted charges [1, y - c] in a copy of
+// the whole grid in shared memory (m planes of N^d floats), and adds the
+// touched nodes to V (zeroed by k_bin_count) with one vector atomic each.
+// The lanes of a warp hold 32 consecutive points.  When they fall in at most
+// four cells (points in a spatial order, the common case after the Morton
+// relabelling), the warp sums each cell's 4^d m values by halving shuffles
+// and distinct lanes publish the totals; otherwise (points scattered over
+// the grid, as early in a run) each lane adds its own values with
+// shared-memory atomics, which then rarely meet on one node.
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ void s2g_direct_warp(float *Vs, int N, int nodes, int key,
+                                                const int *f, const float (*w)[4],
+                                                const float *qc, int lane) {
+  constexpr int NN = D == 1 ? 4 : 16, C = D + 1, K = NN * C;
+  const unsigned full = 0xffffffffu;
+  const unsigned valid = __ballot_sync(full, key >= 0);
+  if (valid == 0u) return;
+  const unsigned grp = __match_any_sync(full, key);
+  const bool leader = key >= 0 && lane == __ffs(grp) - 1;
+  const int ngroups = __popc(__ballot_sync(full, leader));
+  if (ngroups <= 4) {
+    unsigned rem = valid;
+    while (rem) {  // warp-uniform
+      const int l0 = __ffs(rem) - 1;
+      const int gk = __shfl_sync(full, key, l0);
+      const int g0 = __shfl_sync(full, f[0], l0);
+      const int g1 = D == 2 ? __shfl_sync(full, f[1], l0) : 0;
+      const bool in = key == gk;
+      const unsigned gm = __ballot_sync(full, in);
+      float a[K];
+#pragma unroll
+      for (int a1 = 0; a1 < (D == 2 ? 4 : 1); a1++)
+#pragma unroll
+        for (int a0 = 0; a0 < 4; a0++) {
+          const float wt = in ? (D == 2 ? w[1][a1] : 1.f) * w[0][a0] : 0.f;
+          const int nd = a1 * 4 + a0;
+          a[nd * C] = wt;
+#pragma unroll
+          for (int k = 0; k < D; k++) a[nd * C + 1 + k] = wt * qc[k];
+        }
+      int base = 0;
+      warp_multi_sum<K, 16>(a, lane, base);
+      if ((lane & wsum_full_mask(K, 16)) == 0) {
+#pragma unroll
+        for (int q = 0; q < wsum_count(K, 16); q++) {
+          const int idx = base + q, nd = idx / C, ch = idx % C;
+          const int node = g0 + (nd & 3) + (D == 2 ? N * (g1 + (nd >> 2)) : 0);
+          atomicAdd(&Vs[ch * nodes + node], a[q]);
+        }
+      }
+      rem &= ~gm;
+    }
+  } else if (key >= 0) {
+#pragma unroll
+    for (int a1 = 0; a1 < (D == 2 ? 4 : 1); a1++)
+#pragma unroll
+      for (int a0 = 0; a0 < 4; a0++) {
+        const float wt = (D == 2 ? w[1][a1] : 1.f) * w[0][a0];
+        const int node = f[0] + a0 + (D == 2 ? N * (f[1] + a1) : 0);
+        atomicAdd(&Vs[node], wt);
+#pragma unroll
+        for (int k = 0; k < D; k++) atomicAdd(&Vs[(k + 1) * nodes + node], wt * qc[k]);
+      }
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void k_s2g_direct_body(int vb_, int vg_, const typename Vec<D>::T *__restrict__ Y,
+                                                  int n, SgtState *st,
+                                                  typename Node<D>::T *__restrict__ V) {
+  static_assert(D <= 2, "direct mode is for d <= 2");
+  sgt_pdl_wait();
+  if (st->T != 0) return;  // cell and tile modes: the sort and k_s2g* do it
+  extern __shared__ float sgt_direct_grid[];
+  float *Vs = sgt_direct_grid;
+  constexpr int C = D + 1;
+  const int N = st->N, cells = N - 3;
+  const int nodes = D == 1 ? N : N * N;
+  const float maxy = st->maxy, scale = st->scale, hc = 0.5f * maxy;
+  float miny[2];
+#pragma unroll
+  for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  for (int e = threadIdx.x; e < C * nodes; e += blockDim.x) Vs[e] = 0.f;
+  __syncthreads();
+  const int per = (n + vg_ - 1) / vg_;
+  const int lo = vb_ * per, hi = min(n, lo + per);
+  const int lane = threadIdx.x & 31;
+  constexpr int U = SGT_PTS_U;
+  for (int i0 = lo + (threadIdx.x & ~31) * U; i0 < hi; i0 += blockDim.x * U) {
+    typename Vec<D>::T yv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + 32 * u + lane;
+      if (i < hi) yv[u] = Y[i];
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + 32 * u + lane;
+      int key = -1;
+      int f[2] = {0, 0};
+      float w[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}}, qc[2] = {0.f, 0.f};
+      if (i < hi) {
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+          float sh;
+          const float sv = sgt_scale(comp<D>(yv[u], k), miny[k], maxy, scale, sh);
+          sgt_weights(sv, f[k], w[k]);
+          qc[k] = sh - hc;
+        }
+        key = D == 1 ? f[0] : f[0] + cells * f[1];
+        if ((unsigned)f[0] >= (unsigned)cells || (D == 2 && (unsigned)f[1] >= (unsigned)cells)) {
+          atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);  // outside the grid: skip the point
+          key = -1;
+        }
+      }
+      s2g_direct_warp<D>(Vs, N, nodes, key, f, w, qc, lane);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nodes; e += blockDim.x) {
+    const float a0 = Vs[e], a1 = Vs[nodes + e], a2 = D == 2 ? Vs[2 * nodes + e] : 0.f;
+    if (a0 == 0.f && a1 == 0.f && a2 == 0.f) continue;
+    if constexpr (D == 1) atomicAdd(&V[e], make_float2(a0, a1));
+    else atomicAdd(&V[e], make_float4(a0, a1, a2, 0.f));
+  }
+}
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_s2g_direct(const typename Vec<D>::T *__restrict__ Y, int n, SgtState *st,
+             typename Node<D>::T *__restrict__ V) {
+  k_s2g_direct_body<D>(blockIdx.x, gridDim.x, Y, n, st, V);
+}
+
+// ---------------------------------------------------------------------------
 // bin_scatter: counting-sort points into tile order.  Each CTA owns a
 // contiguous range; it counts per tile, reserves its slots with one global
 // atomic per touched tile, then places its points.
@@ -418,6 +587,7 @@ __device__ __forceinline__ void k_bin_scatter_body(int vb_, int vg_, const typen
               int *__restrict__ cursor, float4 *__restrict__ sorted) {
   sgt_pdl_wait();
   __shared__ int lc[SGT_HIST_MAX];
+  if (st->T == 0) return;  // direct mode: k_s2g_direct does the S2G
   const int ntiles = st->ntiles, T = st->T, td = st->tiles_dim;
   const float maxy = st->maxy, scale = st->scale;
   float miny[3];
@@ -788,12 +958,12 @@ k_s2g_cell(const float4 *__restrict__ sorted, SgtState *st,
 }
 
 // Interpolated potentials p[0..d] at a point with stencil weights w and base
-// cell f: from the grid Phi, or (SM) from the block's copy cn of the 4^d nodes
-// of the point's cell, node a0 + 4 a1 + 16 a2.  Same products in the same
-// order either way.
+// cell f: from a grid Phi (in global or shared memory), or (SM) from the
+// block's copy cn of the 4^d nodes of the point's cell, node a0 + 4 a1 +
+// 16 a2.  Same products in the same order either way.
 template <int D, bool SM>
 __device__ __forceinline__ void g2s_potentials(const float (*w)[4], const int *f, int N,
-                                               const typename Node<D>::T *__restrict__ Phi,
+                                               const typename Node<D>::T *Phi,
                                                const typename Node<D>::T *cn, float *p) {
 #pragma unroll
   for (int a2 = 0; a2 < (D >= 3 ? 4 : 1); a2++)
@@ -810,7 +980,7 @@ __device__ __forceinline__ void g2s_potentials(const float (*w)[4], const int *f
         const float wt = wy * w[0][a0];
         typename Node<D>::T v;
         if constexpr (SM) v = cn[a0 + 4 * (a1 + 4 * a2)];
-        else v = __ldg(&Phi[base + a0]);
+        else v = Phi[base + a0];
         p[0] += wt * v.x;
         p[1] += wt * v.y;
         if constexpr (D >= 2) {
@@ -819,6 +989,38 @@ __device__ __forceinline__ void g2s_potentials(const float (*w)[4], const int *f
         }
       }
     }
+}
+
+// Z of a G2S launch: the block's FP64 partial, then the last block to finish
+// sums the partials in block order and writes Z = sum - n.
+__device__ __forceinline__ void g2s_finish(int vb_, int vg_, SgtState *st, double *part_z, int n,
+                                           double zacc, double *wz, bool &last) {
+  zacc = warp_sum_d(zacc);
+  if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = zacc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int k = 0; k < SGT_THREADS / 32; k++) s += wz[k];
+    part_z[vb_] = s;
+    __threadfence();
+    last = (atomicAdd(&st->done_g2s, 1u) == vg_ - 1);
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    double s = 0;
+    for (int b = threadIdx.x; b < (int)vg_; b += blockDim.x) s += __ldcg(&part_z[b]);
+    s = warp_sum_d(s);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0;
+      for (int k = 0; k < SGT_THREADS / 32; k++) t += wz[k];
+      st->Z = t - (double)n;
+      st->done_g2s = 0;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -839,13 +1041,14 @@ __device__ __forceinline__ void k_g2s_body(int vb_, int vg_, const float4 *__res
   float miny[3];
 #pragma unroll
   for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  if (st->T == 0) return;  // direct mode: k_g2s_direct does the G2S
+  double zacc = 0.0;
   // cell mode (T = 1): every point of a chunk reads the same 4^d nodes,
   // which the block stages once per chunk in shared memory
   constexpr int NNODES = D == 1 ? 4 : (D == 2 ? 16 : 64);
   __shared__ typename Node<D>::T cn[NNODES];
   const bool cell = st->T == 1;
   const int td = st->tiles_dim;
-  double zacc = 0.0;
   for (int c = vb_; c < nch; c += vg_) {
     const int4 ch = chunks[c];
     int cf[3] = {-1, -1, -1};
@@ -898,32 +1101,7 @@ __device__ __forceinline__ void k_g2s_body(int vb_, int vg_, const float4 *__res
       }
     }
   }
-  zacc = warp_sum_d(zacc);
-  if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = zacc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0;
-    for (int k = 0; k < SGT_THREADS / 32; k++) s += wz[k];
-    part_z[vb_] = s;
-    __threadfence();
-    last = (atomicAdd(&st->done_g2s, 1u) == vg_ - 1);
-  }
-  __syncthreads();
-  if (last) {
-    __threadfence();
-    double s = 0;
-    for (int b = threadIdx.x; b < (int)vg_; b += blockDim.x) s += __ldcg(&part_z[b]);
-    s = warp_sum_d(s);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) wz[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0;
-      for (int k = 0; k < SGT_THREADS / 32; k++) t += wz[k];
-      st->Z = t - (double)n;
-      st->done_g2s = 0;
-    }
-  }
+  g2s_finish(vb_, vg_, st, part_z, n, zacc, wz, last);
 }
 template <int D>
 __global__ void __launch_bounds__(SGT_THREADS)
@@ -932,6 +1110,82 @@ k_g2s(const float4 *__restrict__ sorted, SgtState *st,
       const typename Node<D>::T *__restrict__ Phi,
       typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n) {
   k_g2s_body<D>(blockIdx.x, gridDim.x, sorted, st, chunks, Phi, Frep_un, part_z, n);
+}
+
+// ---------------------------------------------------------------------------
+// Direct-mode G2S (T = 0): the points in their own order, the whole potential
+// grid staged in shared memory, F written in place (coalesced), Z as in
+// k_g2s.
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ void k_g2s_direct_body(int vb_, int vg_, SgtState *st,
+      const typename Node<D>::T *__restrict__ Phi,
+      typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n,
+      const typename Vec<D>::T *__restrict__ Y) {
+  static_assert(D <= 2, "direct mode is for d <= 2");
+  sgt_pdl_wait();
+  __shared__ double wz[SGT_THREADS / 32];
+  __shared__ bool last;
+  if (st->T != 0) return;  // cell and tile modes: k_g2s does it
+  const int N = st->N;
+  const float maxy = st->maxy, scale = st->scale;
+  const float hc = 0.5f * maxy;
+  float miny[3];
+#pragma unroll
+  for (int k = 0; k < D; k++) miny[k] = st->miny[k];
+  double zacc = 0.0;
+  extern __shared__ float4 sgt_g2s_smem[];
+  typename Node<D>::T *Ps = reinterpret_cast<typename Node<D>::T *>(sgt_g2s_smem);
+  const int nodes = D == 1 ? N : N * N;
+  for (int e = threadIdx.x; e < nodes; e += blockDim.x) Ps[e] = Phi[e];
+  __syncthreads();
+  constexpr int U = SGT_PTS_U;
+  const int lane = threadIdx.x & 31;
+  const long stride = (long)vg_ * blockDim.x * U;
+  for (long i0 = ((long)vb_ * blockDim.x + (threadIdx.x & ~31)) * U; i0 < n; i0 += stride) {
+    typename Vec<D>::T yv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long i = i0 + 32 * u + lane;
+      if (i < n) yv[u] = Y[i];
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long i = i0 + 32 * u + lane;
+      if (i >= n) break;
+      int f[3];
+      float w[3][4], ys[3];
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        const float sv = sgt_scale(comp<D>(yv[u], k), miny[k], maxy, scale, ys[k]);
+        sgt_weights(sv, f[k], w[k]);
+      }
+      float p[4] = {0.f, 0.f, 0.f, 0.f};
+      if ((unsigned)f[0] < (unsigned)(N - 3) && (D == 1 || (unsigned)f[1] < (unsigned)(N - 3)))
+        g2s_potentials<D, false>(w, f, N, Ps, Ps, p);
+      else  // outside the grid (S2G skipped it too): no force, no Z
+        atomicOr(&st->error, SGT_EFLAG_CHUNK_OVERFLOW);
+      double ysq = 0.0, dot = 0.0;
+      typename Vec<D>::T fr;
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        const float yk = ys[k] - hc;
+        ysq += (double)yk * yk;
+        dot += (double)yk * p[k + 1];
+        setcomp<D>(fr, k, yk * p[0] - p[k + 1]);
+      }
+      zacc += (1.0 + 2.0 * ysq) * (double)p[0] - 2.0 * dot;
+      Frep_un[i] = fr;
+    }
+  }
+  g2s_finish(vb_, vg_, st, part_z, n, zacc, wz, last);
+}
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+k_g2s_direct(SgtState *st, const typename Node<D>::T *__restrict__ Phi,
+             typename Vec<D>::T *__restrict__ Frep_un, double *part_z, int n,
+             const typename Vec<D>::T *__restrict__ Y) {
+  k_g2s_direct_body<D>(blockIdx.x, gridDim.x, st, Phi, Frep_un, part_z, n, Y);
 }
 
 // ---------------------------------------------------------------------------

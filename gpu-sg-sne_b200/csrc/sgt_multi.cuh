@@ -66,6 +66,14 @@ km_bin_scatter(const SgtJobView *__restrict__ views, const int *__restrict__ pre
   k_bin_scatter_body<D>(vb, vg, (const typename Vec<D>::T *)v.Y, v.n, v.st, v.cursor, v.sorted);
 }
 
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+km_s2g_direct(const SgtJobView *__restrict__ views, const int *__restrict__ prefix, int njobs) {
+  SGT_MULTI_JOB
+  k_s2g_direct_body<D>(vb, vg, (const typename Vec<D>::T *)v.Y, v.n, v.st,
+                       (typename Node<D>::T *)v.V);
+}
+
 template <int D, int TT>
 __global__ void __launch_bounds__(SGT_THREADS)
 km_s2g(const SgtJobView *__restrict__ views, const int *__restrict__ prefix, int njobs) {
@@ -115,6 +123,15 @@ km_g2s(const SgtJobView *__restrict__ views, const int *__restrict__ prefix, int
   typedef typename Vec<D>::T VT;
   k_g2s_body<D>(vb, vg, v.sorted, v.st, v.chunks, (const typename Node<D>::T *)v.Phi,
                 (VT *)v.Frep, v.part_z, v.n);
+}
+
+template <int D>
+__global__ void __launch_bounds__(SGT_THREADS)
+km_g2s_direct(const SgtJobView *__restrict__ views, const int *__restrict__ prefix, int njobs) {
+  SGT_MULTI_JOB
+  typedef typename Vec<D>::T VT;
+  k_g2s_direct_body<D>(vb, vg, v.st, (const typename Node<D>::T *)v.Phi, (VT *)v.Frep, v.part_z,
+                       v.n, (const VT *)v.Y);
 }
 
 template <int D, int G>

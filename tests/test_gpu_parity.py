@@ -161,6 +161,44 @@ def test_cell_mode_vs_oracle(torch, ctx, oracle, d, kind):
     assert rel(F, Fo) <= 3e-4
 
 
+@pytest.mark.parametrize("kind", ["clusters", "compact", "ordered"])
+@pytest.mark.parametrize("ng", [58, 66])
+def test_direct_and_sorted_modes_2d(torch, ctx, oracle, kind, ng):
+    """2-D grids too sparse for cell mode, on either side of the direct-mode
+    limit (64 points per axis): fixed grid 58 -> N = 60 takes the direct mode
+    (S2G in shared memory over the points in their own order), 66 -> N = 70
+    the tile sort.  Points in
+    clusters, compact, and sorted along a space-filling order (the warp
+    reduction of the direct S2G); charge grid, forces and Z against the
+    oracle."""
+    import sgtsne_b200 as S
+    n, d, h = 40000, 2, 0.7
+    rng = np.random.default_rng(77 + ng)
+    if kind == "compact":
+        Y = (rng.standard_normal((n, d)) * 1.5).astype(np.float32)
+    else:
+        c = rng.standard_normal((6, d)) * 3
+        Y = (c[rng.integers(0, 6, n)] + rng.standard_normal((n, d)) * 0.3).astype(np.float32)
+    if kind == "ordered":  # runs of points in one cell, as after a relabelling
+        q = np.floor((Y - Y.min(0)) / 0.25).astype(np.int64)
+        Y = Y[np.lexsort((q[:, 0], q[:, 1]))]
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    Z, N, he = ctx.repulsive(n, d, h, ng, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    assert N == oracle.best_grid_size(ng) + 2
+    V, Phi = ctx.last_grids(d, N)
+    _, sc, sh, N2, mx = oracle.bins_f32(Y, h, oracle.best_grid_size(ng))
+    assert N2 == N
+    hc = np.float32(0.5) * np.float32(mx)
+    q = np.concatenate([np.ones((n, 1)), (sh - hc).astype(np.float64)], 1)
+    Vo = oracle.s2g(sc.astype(np.float64), q, N)
+    assert rel(V, Vo) <= 1e-5
+    F = f.cpu().numpy().reshape(n, d)
+    Fo, Zo, No, heo = oracle.repulsive_interp(Y.astype(np.float64), h, n1_force=N - 2)
+    assert No == N
+    assert abs(Z - Zo) <= 5e-4 * abs(Zo)
+    assert rel(F, Fo) <= 3e-4
+
+
 @pytest.mark.parametrize("fmt", [0, 2, 3])
 @pytest.mark.parametrize("d", [1, 2, 3])
 def test_attractive_formats(torch, ctx, oracle, fmt, d):
