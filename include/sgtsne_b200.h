@@ -110,6 +110,11 @@ typedef struct sgt_job sgt_job;
 int sgt_abi_version(void);
 const char *sgt_status_string(sgt_status s);
 
+/* A context owns a stream and a stream-ordered device memory pool: jobs and
+   operator calls allocate from it, and memory a retired job frees stays in
+   the pool for the next job (no new pages are mapped).  sgt_destroy returns
+   the pool's memory to the driver (buffers of jobs still alive are released
+   when those jobs are destroyed). */
 sgt_status sgt_create(int device, sgt_ctx **out);
 void sgt_destroy(sgt_ctx *ctx);
 /* Queue all work of ctx on a caller-owned cudaStream_t (NULL = own stream). */
