@@ -199,6 +199,34 @@ def test_direct_and_sorted_modes_2d(torch, ctx, oracle, kind, ng):
     assert rel(F, Fo) <= 3e-4
 
 
+@pytest.mark.parametrize("ng", [20, 40])
+def test_dense_job_modes_2d(torch, ctx, oracle, ng):
+    """A 2-D job with enough points (2.6M) that its grids up to 64 points per
+    axis are all dense never takes the direct mode: fixed grids 20 -> N = 25
+    and 40 -> N = 42 run in cell mode, with many chunks per cell.  Charge
+    grid, forces and Z against the oracle."""
+    import sgtsne_b200 as S
+    n, d, h = 2600000, 2, 0.7
+    rng = np.random.default_rng(90 + ng)
+    c = rng.standard_normal((6, d)) * 3
+    Y = (c[rng.integers(0, 6, n)] + rng.standard_normal((n, d)) * 0.5).astype(np.float32)
+    f = torch.empty(n * d, dtype=torch.float32, device="cuda")
+    Z, N, he = ctx.repulsive(n, d, h, ng, dev(torch, Y), S.LAYOUT_POINT_MAJOR, f)
+    assert N == oracle.best_grid_size(ng) + 2
+    V, Phi = ctx.last_grids(d, N)
+    _, sc, sh, N2, mx = oracle.bins_f32(Y, h, oracle.best_grid_size(ng))
+    assert N2 == N
+    hc = np.float32(0.5) * np.float32(mx)
+    q = np.concatenate([np.ones((n, 1)), (sh - hc).astype(np.float64)], 1)
+    Vo = oracle.s2g(sc.astype(np.float64), q, N)
+    assert rel(V, Vo) <= 1e-5
+    F = f.cpu().numpy().reshape(n, d)
+    Fo, Zo, No, heo = oracle.repulsive_interp(Y.astype(np.float64), h, n1_force=N - 2)
+    assert No == N
+    assert abs(Z - Zo) <= 5e-4 * abs(Zo)
+    assert rel(F, Fo) <= 3e-4
+
+
 @pytest.mark.parametrize("fmt", [0, 2, 3])
 @pytest.mark.parametrize("d", [1, 2, 3])
 def test_attractive_formats(torch, ctx, oracle, fmt, d):
