@@ -546,6 +546,17 @@ def run_ours(args, rank, world, local, dist):
                          "algorithmic_bytes_per_launch": alg,
                          "traffic": None if ratio is None else ratio * alg},
             "e2e": e2e,
+            # the engine has one arithmetic form (FP32 SpMV, scatter, FFT and
+            # gather; FP64 Z, KL and row sums), the precision form of the
+            # north star without its optional split-BF16 DFT-GEMM convolution;
+            # the convolution's share bounds what a faster convolution can give
+            "precision": {
+                "form": "FP32 SpMV/S2G/FFT/G2S with FP32 accumulation; FP64 Z, KL, row sums",
+                "split_bf16_dft_gemm_convolution": "not built",
+                "convolution_ms": round(stage_avg[2], 4),
+                "convolution_share_of_serial_iteration": round(stage_avg[2] / stage_avg[5], 4),
+                "iteration_speedup_if_convolution_were_free":
+                    round(1.0 / (1.0 - stage_avg[2] / stage_avg[5]), 4)},
             "gpu_launches": launches,
             "clocks": clk,
             "knn_compare": knn_cmp,
@@ -757,6 +768,9 @@ def main():
                 threads = os.cpu_count() or 1
                 # the checker at full size, then the CPU baseline sample
                 out["parity"] = parity_check(srp, sc, sv, pstate, threads)
+                par = out["parity"] or {}
+                out["precision"]["error_vs_fp64"] = {
+                    k: par.get(k) for k in ("f_attr_rel_l2", "f_rep_rel_l2", "z_rel")}
                 spi, _ = cpu_sample(srp, sc, sv, pstate["y"], args.cpu_iters, threads)
                 out["cpu_baseline"] = {"value": 1.0 / spi, "unit": "iters/s", "cores": threads,
                                        "kind": "port",
